@@ -1,0 +1,333 @@
+// Receptor grid maps (sm_100a): Vina/Vinardo per-ligand-type maps and the fitted function's maps.
+//
+// The reference launches one thread per grid point that scans every receptor atom (grid.py:24-61,
+// gridfit.py:21-57). Here a 128-thread CTA owns a 4 x 4 x 8 tile of points (z fastest, one warp per x-plane
+// patch). The CTA streams the receptor atoms with coalesced loads, keeps those inside the tile's bounding box
+// grown by the cutoff in shared memory (ordered compaction, so every point still sums its atoms in receptor
+// index order, as the reference does), and each thread then evaluates its point against the staged atoms.
+// Unweighted term sums are kept per type in registers (groups of 8 types) and weighted once at the end, the
+// same order of operations as the reference kernel.
+#include "common.cuh"
+
+namespace adock {
+
+#define TILE_X 4
+#define TILE_Y 4
+#define TILE_Z 8
+#define TILE_THREADS 128
+#define STAGE_CAP 2048
+#define VINA_GROUP 8
+#define FIT_GROUP 8
+
+struct VinaPrm {
+    float cutoff, g1_off, g1_inv, g2_off, g2_inv, rep_off, hyd_good, hyd_bad, hyd_inv, hb_good, hb_bad, hb_inv;
+    float w[5];
+    int n_lt, n_xs, per_term;
+    int lig_types[24];
+    float radius[64];
+    int flags[64];  // bit0 hydrophobic, bit1 donor, bit2 acceptor
+};
+
+struct FitPrm {
+    float cutoff, g1_off, g1_inv, g2_off, g2_inv, rep_off, hyd_good, hyd_bad, hyd_inv, hb_good, hb_bad, hb_inv;
+    float ion_rmin, rep_cap;
+    int n_lt, n_rt;
+    float rad_lig[64];
+};
+
+// Stage the receptor atoms inside [lo, hi] (per axis) from index `start`; returns the index where staging
+// stopped (n_rec when all atoms were seen). Order of the staged atoms = receptor index order.
+__device__ __forceinline__ int stage_atoms(const float* __restrict__ rxyz, const int* __restrict__ rtype, int n_rec,
+                                           int start, const float* lo, const float* hi, float4* S, int* count,
+                                           int* wsum) {
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    int n = 0;
+    int a0 = start;
+    for (; a0 < n_rec; a0 += TILE_THREADS) {
+        if (n + TILE_THREADS > STAGE_CAP) break;
+        const int a = a0 + tid;
+        bool in = false;
+        float x = 0.f, y = 0.f, z = 0.f;
+        int t = 0;
+        if (a < n_rec) {
+            x = rxyz[3 * a]; y = rxyz[3 * a + 1]; z = rxyz[3 * a + 2];
+            t = rtype[a];
+            in = !(x < lo[0] || x > hi[0] || y < lo[1] || y > hi[1] || z < lo[2] || z > hi[2]);
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, in);
+        if (lane == 0) wsum[wid] = __popc(bal);
+        __syncthreads();
+        int off = n;
+        for (int w = 0; w < wid; ++w) off += wsum[w];
+        if (in) S[off + __popc(bal & ((1u << lane) - 1u))] = make_float4(x, y, z, __int_as_float(t));
+        int tot = 0;
+        for (int w = 0; w < TILE_THREADS / 32; ++w) tot += wsum[w];
+        n += tot;
+        __syncthreads();
+    }
+    *count = n;
+    return a0 < n_rec ? a0 : n_rec;
+}
+
+__global__ void __launch_bounds__(TILE_THREADS) grid_vina_kernel(const float* __restrict__ rxyz,
+                                                                 const int* __restrict__ rtype, int n_rec, float ox,
+                                                                 float oy, float oz, float spacing, int nx, int ny,
+                                                                 int nz, const __grid_constant__ VinaPrm P,
+                                                                 float* __restrict__ out) {
+    __shared__ float4 S[STAGE_CAP];
+    __shared__ int wsum[TILE_THREADS / 32];
+    const int tx = blockIdx.x, ty = blockIdx.y, tz = blockIdx.z;
+    const int tid = threadIdx.x;
+    const int k = tz * TILE_Z + (tid % TILE_Z);
+    const int j = ty * TILE_Y + (tid / TILE_Z) % TILE_Y;
+    const int i = tx * TILE_X + tid / (TILE_Z * TILE_Y);
+    const bool valid = i < nx && j < ny && k < nz;
+    const float x = ox + i * spacing, y = oy + j * spacing, z = oz + k * spacing;
+    const int i1 = min(tx * TILE_X + TILE_X, nx), j1 = min(ty * TILE_Y + TILE_Y, ny), k1 = min(tz * TILE_Z + TILE_Z, nz);
+    const float cut = P.cutoff, cut2 = cut * cut;
+    const float lo[3] = {ox + tx * TILE_X * spacing - cut, oy + ty * TILE_Y * spacing - cut, oz + tz * TILE_Z * spacing - cut};
+    const float hi[3] = {ox + (i1 - 1) * spacing + cut, oy + (j1 - 1) * spacing + cut, oz + (k1 - 1) * spacing + cut};
+    const long long npts = (long long)nx * ny * nz;
+    const long long p = ((long long)i * ny + j) * nz + k;
+
+    for (int q0 = 0; q0 < P.n_lt; q0 += VINA_GROUP) {
+        float acc[VINA_GROUP][5];
+#pragma unroll
+        for (int q = 0; q < VINA_GROUP; ++q)
+#pragma unroll
+            for (int m = 0; m < 5; ++m) acc[q][m] = 0.f;
+        float rl[VINA_GROUP];
+        int fl[VINA_GROUP];
+#pragma unroll
+        for (int q = 0; q < VINA_GROUP; ++q) {
+            const int tl = (q0 + q < P.n_lt) ? P.lig_types[q0 + q] : 0;
+            rl[q] = P.radius[tl];
+            fl[q] = P.flags[tl];
+        }
+        int start = 0;
+        while (start < n_rec) {
+            int cnt;
+            start = stage_atoms(rxyz, rtype, n_rec, start, lo, hi, S, &cnt, wsum);
+            if (valid) {
+                for (int s = 0; s < cnt; ++s) {
+                    const float4 A = S[s];
+                    const float dx = A.x - x, dy = A.y - y, dz = A.z - z;
+                    const float r2 = dx * dx + dy * dy + dz * dz;
+                    if (r2 >= cut2) continue;
+                    const float r = sqrtf(r2);
+                    const int ta = __float_as_int(A.w);
+                    const float ra = P.radius[ta];
+                    const int fa = P.flags[ta];
+#pragma unroll
+                    for (int q = 0; q < VINA_GROUP; ++q) {
+                        if (q0 + q < P.n_lt) {
+                            const float d = r - ra - rl[q];
+                            float u = (d - P.g1_off) * P.g1_inv;
+                            const float g1 = expf(-u * u);
+                            u = (d - P.g2_off) * P.g2_inv;
+                            const float g2 = expf(-u * u);
+                            const float dr = d - P.rep_off;
+                            const float rep = dr < 0.f ? dr * dr : 0.f;
+                            float hy = 0.f, hb = 0.f;
+                            if ((fa & 1) && (fl[q] & 1)) hy = fminf(fmaxf((P.hyd_bad - d) * P.hyd_inv, 0.f), 1.f);
+                            if (((fa & 2) && (fl[q] & 4)) || ((fa & 4) && (fl[q] & 2)))
+                                hb = fminf(fmaxf((P.hb_bad - d) * P.hb_inv, 0.f), 1.f);
+                            acc[q][0] += g1; acc[q][1] += g2; acc[q][2] += rep; acc[q][3] += hy; acc[q][4] += hb;
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        if (valid) {
+#pragma unroll
+            for (int q = 0; q < VINA_GROUP; ++q) {
+                const int qq = q0 + q;
+                if (qq >= P.n_lt) break;
+                if (P.per_term) {
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) out[((long long)(m * P.n_lt + qq)) * npts + p] = acc[q][m];
+                } else {
+                    float e = 0.f;
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) e += P.w[m] * acc[q][m];
+                    out[(long long)qq * npts + p] = e;
+                }
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(TILE_THREADS) grid_fit_kernel(const float* __restrict__ rxyz,
+                                                                const int* __restrict__ rext, int n_rec, float ox,
+                                                                float oy, float oz, float spacing, int nx, int ny,
+                                                                int nz, const __grid_constant__ FitPrm P,
+                                                                const float* __restrict__ W, const float* __restrict__ rad_rec,
+                                                                float* __restrict__ out) {
+    __shared__ float4 S[STAGE_CAP];
+    __shared__ int wsum[TILE_THREADS / 32];
+    extern __shared__ float Wsh[];   // [n_rt, FIT_GROUP, 6] slice of W, then rad_rec [n_rt]
+    float* Rsh = Wsh + (size_t)P.n_rt * FIT_GROUP * 6;
+    const int tx = blockIdx.x, ty = blockIdx.y, tz = blockIdx.z;
+    const int tid = threadIdx.x;
+    const int k = tz * TILE_Z + (tid % TILE_Z);
+    const int j = ty * TILE_Y + (tid / TILE_Z) % TILE_Y;
+    const int i = tx * TILE_X + tid / (TILE_Z * TILE_Y);
+    const bool valid = i < nx && j < ny && k < nz;
+    const float x = ox + i * spacing, y = oy + j * spacing, z = oz + k * spacing;
+    const int i1 = min(tx * TILE_X + TILE_X, nx), j1 = min(ty * TILE_Y + TILE_Y, ny), k1 = min(tz * TILE_Z + TILE_Z, nz);
+    const float rc = P.cutoff, cut2 = rc * rc;
+    const float lo[3] = {ox + tx * TILE_X * spacing - rc, oy + ty * TILE_Y * spacing - rc, oz + tz * TILE_Z * spacing - rc};
+    const float hi[3] = {ox + (i1 - 1) * spacing + rc, oy + (j1 - 1) * spacing + rc, oz + (k1 - 1) * spacing + rc};
+    const long long npts = (long long)nx * ny * nz;
+    const long long p = ((long long)i * ny + j) * nz + k;
+    for (int t = tid; t < P.n_rt; t += TILE_THREADS) Rsh[t] = rad_rec[t];
+
+    for (int q0 = 0; q0 < P.n_lt; q0 += FIT_GROUP) {
+        const int gq = min(FIT_GROUP, P.n_lt - q0);
+        __syncthreads();
+        for (int e = tid; e < P.n_rt * FIT_GROUP * 6; e += TILE_THREADS) {
+            const int t = e / (FIT_GROUP * 6), q = (e / 6) % FIT_GROUP, b = e % 6;
+            Wsh[e] = q < gq ? W[((long long)t * P.n_lt + q0 + q) * 6 + b] : 0.f;
+        }
+        __syncthreads();
+        float acc[FIT_GROUP];
+        float rl[FIT_GROUP];
+#pragma unroll
+        for (int q = 0; q < FIT_GROUP; ++q) {
+            acc[q] = 0.f;
+            rl[q] = q < gq ? P.rad_lig[q0 + q] : 0.f;
+        }
+        int start = 0;
+        while (start < n_rec) {
+            int cnt;
+            start = stage_atoms(rxyz, rext, n_rec, start, lo, hi, S, &cnt, wsum);
+            if (valid) {
+                for (int s = 0; s < cnt; ++s) {
+                    const float4 A = S[s];
+                    const float dx = A.x - x, dy = A.y - y, dz = A.z - z;
+                    const float r2 = dx * dx + dy * dy + dz * dz;
+                    if (r2 >= cut2) continue;
+                    const float r = sqrtf(r2);
+                    const int ta = __float_as_int(A.w);
+                    const float ra = Rsh[ta];
+                    const float rr = fmaxf(r, P.ion_rmin);
+                    const float ion = 1.f / (rr * rr) - 1.f / cut2;
+                    const float* Wa = Wsh + (size_t)ta * FIT_GROUP * 6;
+#pragma unroll
+                    for (int q = 0; q < FIT_GROUP; ++q) {
+                        if (q < gq) {
+                            const float* w = Wa + q * 6;
+                            const float d = r - ra - rl[q];
+                            float u = (d - P.g1_off) * P.g1_inv;
+                            float s_ = w[0] * expf(-u * u);
+                            u = (d - P.g2_off) * P.g2_inv;
+                            s_ += w[1] * expf(-u * u);
+                            const float dr = d - P.rep_off;
+                            if (dr < 0.f) s_ += w[2] * fminf(dr * dr, P.rep_cap);
+                            s_ += w[3] * fminf(fmaxf((P.hyd_bad - d) * P.hyd_inv, 0.f), 1.f);
+                            s_ += w[4] * fminf(fmaxf((P.hb_bad - d) * P.hb_inv, 0.f), 1.f);
+                            s_ += w[5] * ion;
+                            acc[q] += s_;
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        if (valid) {
+#pragma unroll
+            for (int q = 0; q < FIT_GROUP; ++q)
+                if (q < gq) out[(long long)(q0 + q) * npts + p] = acc[q];
+        }
+    }
+}
+
+template <typename T>
+__global__ void convert_kernel(const float* __restrict__ src, T* __restrict__ dst, long long n);
+template <>
+__global__ void convert_kernel<__half>(const float* __restrict__ src, __half* __restrict__ dst, long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = __float2half_rn(src[i]);
+}
+template <>
+__global__ void convert_kernel<__nv_bfloat16>(const float* __restrict__ src, __nv_bfloat16* __restrict__ dst, long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = __float2bfloat16_rn(src[i]);
+}
+
+}  // namespace adock
+
+using namespace adock;
+
+extern "C" int adock_grid_vina(const float* rec_xyz, const int* rec_types, int n_rec, const float* radius,
+                               const int* hyd, const int* don, const int* acc, int n_xs, const int* lig_types,
+                               int n_lt, float ox, float oy, float oz, float spacing, int nx, int ny, int nz,
+                               const float* prm, int per_term, float* out, void* stream) {
+    ADOCK_CHECK_ARG(n_rec >= 0 && (n_rec == 0 || (rec_xyz && rec_types)), "bad receptor arrays");
+    ADOCK_CHECK_ARG(radius && hyd && don && acc && lig_types && prm && out, "null argument");
+    ADOCK_CHECK_ARG(n_xs >= 1 && n_xs <= 64, "n_xs must be in [1, 64] (got %d)", n_xs);
+    ADOCK_CHECK_ARG(n_lt >= 1 && n_lt <= 24, "n_lt must be in [1, 24] (got %d)", n_lt);
+    ADOCK_CHECK_ARG(nx >= 1 && ny >= 1 && nz >= 1, "grid dimensions must be >= 1");
+    ADOCK_CHECK_ARG(spacing > 0.f, "spacing must be > 0");
+    VinaPrm P;
+    P.cutoff = prm[0];
+    P.g1_off = prm[1]; P.g1_inv = 1.f / prm[2]; P.g2_off = prm[3]; P.g2_inv = 1.f / prm[4]; P.rep_off = prm[5];
+    P.hyd_good = prm[6]; P.hyd_bad = prm[7]; P.hyd_inv = 1.f / (prm[7] - prm[6]);
+    P.hb_good = prm[8]; P.hb_bad = prm[9]; P.hb_inv = 1.f / (prm[9] - prm[8]);
+    for (int m = 0; m < 5; ++m) P.w[m] = prm[10 + m];
+    P.n_lt = n_lt; P.n_xs = n_xs; P.per_term = per_term ? 1 : 0;
+    for (int q = 0; q < 24; ++q) P.lig_types[q] = q < n_lt ? lig_types[q] : 0;
+    for (int q = 0; q < n_lt; ++q) ADOCK_CHECK_ARG(lig_types[q] >= 0 && lig_types[q] < n_xs, "ligand type out of range");
+    for (int t = 0; t < 64; ++t) {
+        P.radius[t] = t < n_xs ? radius[t] : 0.f;
+        P.flags[t] = t < n_xs ? ((hyd[t] ? 1 : 0) | (don[t] ? 2 : 0) | (acc[t] ? 4 : 0)) : 0;
+    }
+    dim3 grid((nx + TILE_X - 1) / TILE_X, (ny + TILE_Y - 1) / TILE_Y, (nz + TILE_Z - 1) / TILE_Z);
+    ADOCK_CHECK_ARG(grid.y < 65536 && grid.z < 65536, "grid too large");
+    grid_vina_kernel<<<grid, TILE_THREADS, 0, (cudaStream_t)stream>>>(rec_xyz, rec_types, n_rec, ox, oy, oz, spacing, nx,
+                                                                       ny, nz, P, out);
+    ADOCK_CUDA(cudaGetLastError());
+    return ADOCK_OK;
+}
+
+extern "C" int adock_grid_fit(const float* rec_xyz, const int* rec_ext, int n_rec, const float* rad_rec, int n_rt,
+                              const float* rad_lig, int n_lt, const float* W, float ox, float oy, float oz,
+                              float spacing, int nx, int ny, int nz, const float* prm, float* out, void* stream) {
+    ADOCK_CHECK_ARG(n_rec >= 0 && (n_rec == 0 || (rec_xyz && rec_ext)), "bad receptor arrays");
+    ADOCK_CHECK_ARG(rad_rec && rad_lig && W && prm && out, "null argument");
+    ADOCK_CHECK_ARG(n_lt >= 1 && n_lt <= 64, "n_lt must be in [1, 64] (got %d)", n_lt);
+    ADOCK_CHECK_ARG(n_rt >= 1 && n_rt <= 1024, "n_rt must be in [1, 1024] (got %d)", n_rt);
+    ADOCK_CHECK_ARG(nx >= 1 && ny >= 1 && nz >= 1, "grid dimensions must be >= 1");
+    ADOCK_CHECK_ARG(spacing > 0.f, "spacing must be > 0");
+    FitPrm P;
+    P.cutoff = prm[0];
+    P.g1_off = prm[1]; P.g1_inv = 1.f / prm[2]; P.g2_off = prm[3]; P.g2_inv = 1.f / prm[4]; P.rep_off = prm[5];
+    P.hyd_good = prm[6]; P.hyd_bad = prm[7]; P.hyd_inv = 1.f / (prm[7] - prm[6]);
+    P.hb_good = prm[8]; P.hb_bad = prm[9]; P.hb_inv = 1.f / (prm[9] - prm[8]);
+    P.ion_rmin = prm[10]; P.rep_cap = prm[11];
+    P.n_lt = n_lt; P.n_rt = n_rt;
+    for (int q = 0; q < 64; ++q) P.rad_lig[q] = q < n_lt ? rad_lig[q] : 0.f;
+    const size_t smem = ((size_t)n_rt * FIT_GROUP * 6 + n_rt) * sizeof(float);
+    ADOCK_CUDA(cudaFuncSetAttribute(grid_fit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid((nx + TILE_X - 1) / TILE_X, (ny + TILE_Y - 1) / TILE_Y, (nz + TILE_Z - 1) / TILE_Z);
+    ADOCK_CHECK_ARG(grid.y < 65536 && grid.z < 65536, "grid too large");
+    grid_fit_kernel<<<grid, TILE_THREADS, smem, (cudaStream_t)stream>>>(rec_xyz, rec_ext, n_rec, ox, oy, oz, spacing, nx,
+                                                                          ny, nz, P, W, rad_rec, out);
+    ADOCK_CUDA(cudaGetLastError());
+    return ADOCK_OK;
+}
+
+extern "C" int adock_grid_convert(const float* src, void* dst, long long n, int dtype, void* stream) {
+    ADOCK_CHECK_ARG(src && dst && n >= 0, "bad argument");
+    if (n == 0) return ADOCK_OK;
+    const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148LL * 32);
+    if (dtype == ADOCK_GRID_F16)
+        convert_kernel<__half><<<blocks, 256, 0, (cudaStream_t)stream>>>(src, (__half*)dst, n);
+    else if (dtype == ADOCK_GRID_BF16)
+        convert_kernel<__nv_bfloat16><<<blocks, 256, 0, (cudaStream_t)stream>>>(src, (__nv_bfloat16*)dst, n);
+    else
+        ADOCK_CHECK_ARG(false, "dtype must be ADOCK_GRID_F16 or ADOCK_GRID_BF16");
+    ADOCK_CUDA(cudaGetLastError());
+    return ADOCK_OK;
+}

@@ -1,0 +1,220 @@
+"""``B200KernelProblem``: drop-in for the reference ``KernelProblem`` (``src/adock/mckernel.py:602-726``).
+
+Same constructor argument (a Problem), same attributes (``AM, KM, L, SD, DM``) and the same methods
+(``pack``, ``unpack``, ``energy_grad``, ``receptor_neighbours``, ``stage_a``, ``run_mc``) with the same array
+layouts; the work runs in the sm_100a kernels of ``libadock_b200.so`` through its C-ABI. Errors are raised as
+``RuntimeError`` (argument checks of the C-ABI) or ``AssertionError`` (layout checks, as in the reference).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+from .problem import pack_host
+
+
+class B200KernelProblem:
+    """Packs a batch (ligand preps + GridSet + pair potential) into device arrays for the search kernels.
+
+    State layout per chain: [t(3), q(4) (w,x,y,z), theta(KM)], theta in LigandBatch torsion order.
+    ``grid_dtype``: 'f32', 'f16' or 'bf16' storage of the maps read by the search (FP32 interpolation)."""
+
+    def __init__(self, prob, grid_dtype="f32"):
+        self.AM, self.KM, lig, sf = pack_host(prob)
+        AM, KM, L = self.AM, self.KM, prob.lb.L
+        dev = prob.gs.origin.device
+        if dev.type != "cuda":
+            raise RuntimeError("B200KernelProblem needs CUDA tensors (there is no CPU path)")
+        self.device = dev
+        _lib.load()
+        T = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
+        ref, typ, tm, ax, axp, axu, pr, na, nt, npairs, rg, P, gsl = lig
+        self.P = int(P)
+        self.t_lig = [T(ref), T(typ), T(tm), T(ax), T(axp), T(axu), T(pr), T(na), T(nt), T(npairs), T(rg), T(gsl),
+                      prob.rec_idx.to(device=dev, dtype=torch.int32).contiguous()]
+        self.na_host, self.nt_host = na.copy(), nt.copy()
+        lt = _lib.Ligands()
+        for name, t in zip(("ref", "typ", "tm", "ax", "axp", "axu", "pr", "na", "nt", "np", "rg", "gslot", "rec_idx"),
+                           self.t_lig):
+            setattr(lt, name, _lib.ptr(t))
+        lt.L, lt.AM, lt.KM, lt.P = L, AM, KM, self.P
+        self.c_lig = lt
+        # scoring tables
+        sfp = dict(prob.pot.p)
+        sfp.setdefault("radius", sf[1])
+        sfp.setdefault("hydrophobic", sf[2])
+        sfp.setdefault("donor", sf[3])
+        sfp.setdefault("acceptor", sf[4])
+        self.c_sf = _lib.make_sf(sfp)
+        # grids
+        gs = prob.gs
+        self.grid_dtype = grid_dtype
+        flat, code = gs.storage(grid_dtype)
+        self.t_grid = [flat, gs.offs.to(dev, torch.int64).contiguous(), gs.dims.to(dev, torch.int64).contiguous(),
+                       gs.origin.float().contiguous(), gs.lo.float().contiguous(), gs.hi.float().contiguous()]
+        g = _lib.Grids()
+        g.flat, g.offs, g.dims, g.origin, g.lo, g.hi = [_lib.ptr(t) for t in self.t_grid]
+        g.R, g.dtype, g.spacing, g.penalty = int(gs.origin.shape[0]), code, float(gs.spacing), float(gs.penalty)
+        self.c_grids = g
+        # receptor atoms for exact mode
+        r = _lib.Receptors()
+        if prob.rec is not None:
+            rx, rt, rm = prob.rec
+            self.t_rec = [rx.float().to(dev).contiguous(), rt.to(dev, torch.int32).contiguous(),
+                          rm.sum(1).to(dev, torch.int32).contiguous()]
+            r.xyz, r.typ, r.n = [_lib.ptr(t) for t in self.t_rec]
+            r.RN = int(rx.shape[1])
+        else:
+            self.t_rec = []
+            r.xyz = r.typ = r.n = None
+            r.RN = 0
+        self.c_rec = r
+        # B200 working layout
+        self.t_work = [torch.empty(L * AM * 4, dtype=torch.float32, device=dev),
+                       torch.empty(L * AM, dtype=torch.int32, device=dev),
+                       torch.empty(L * KM * 2 * 4, dtype=torch.float32, device=dev),
+                       torch.empty(L * self.P * 2, dtype=torch.int32, device=dev),
+                       torch.empty(L * 4, dtype=torch.int32, device=dev),
+                       torch.empty(L, dtype=torch.float32, device=dev)]
+        w = _lib.Work()
+        w.atoms, w.masks, w.tors, w.pairs, w.info, w.rg = [_lib.ptr(t) for t in self.t_work]
+        self.c_work = w
+        self.queue = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.evals = torch.zeros(1, dtype=torch.int64, device=dev)
+        with torch.cuda.device(dev):
+            _lib.call("adock_prepare", self.c_lig, self.c_sf, self.c_work, _lib.stream_ptr())
+        self.L, self.SD, self.DM = L, 7 + KM, 6 + KM
+
+    # ---- state packing ----
+    def pack(self, t, q, theta):
+        """t [N,3], q [N,4], theta [N,K<=KM] -> state [N, SD] float32 contiguous."""
+        N, K = theta.shape
+        s = torch.zeros(N, self.SD, device=t.device, dtype=torch.float32)
+        s[:, :3], s[:, 3:7] = t, q
+        s[:, 7:7 + min(K, self.KM)] = theta[:, :self.KM]
+        return s.contiguous()
+
+    def unpack(self, s, K):
+        th = torch.zeros(s.shape[0], K, device=s.device, dtype=s.dtype)
+        th[:, :min(K, self.KM)] = s[:, 7:7 + min(K, self.KM)]
+        th = torch.remainder(th + math.pi, 2 * math.pi) - math.pi
+        return s[:, :3].clone(), s[:, 3:7] / s[:, 3:7].norm(dim=-1, keepdim=True), th
+
+    def _i32(self, x):
+        return x.to(device=self.device, dtype=torch.int32).contiguous()
+
+    # ---- kernels ----
+    def energy_grad(self, chain_lig, state, exact=False):
+        """chain_lig int32 [N], state [N, SD] -> (e [N], g [N, DM])."""
+        N = state.shape[0]
+        e = torch.zeros(N, device=self.device)
+        g = torch.zeros(N, self.DM, device=self.device)
+        if exact:
+            assert self.c_rec.RN > 0, "exact mode needs receptor atoms (Problem.rec)"
+        cl = self._i32(chain_lig)
+        st = state.to(self.device, torch.float32).contiguous()
+        with torch.cuda.device(self.device):
+            _lib.call("adock_eg", self.c_lig, self.c_work, self.c_grids, self.c_sf, self.c_rec, _lib.ptr(cl), N,
+                      _lib.ptr(st), _lib.ptr(e), _lib.ptr(g), int(exact), _lib.stream_ptr())
+        return e, g
+
+    def chain_order(self, chain_lig):
+        """Processing order for the persistent MC kernel: most expensive chains first (cost ~ BFGS iterations x
+        (atoms + pairs / 32))."""
+        cl = chain_lig.long()
+        if not hasattr(self, "_cost"):
+            na = torch.as_tensor(self.na_host, device=self.device).float()
+            npr = self.t_lig[9].float()
+            self._cost = (25 + na) / 3 * (na + npr / 16 + 8)
+        return torch.argsort(-self._cost[cl], stable=True).to(torch.int32)
+
+    def run_mc(self, chain_lig, chain_id, cur, cur_e, best, best_e, init_opt, mc_steps, bfgs_iters, temp,
+               amp_pos, amp_rot, seed, step_offset, exact=False, nbr=None, nbr_n=None, order=None):
+        """In place on cur/cur_e/best/best_e (float32 contiguous CUDA tensors). exact=True with nbr [N, NB] int32 /
+        nbr_n [N]: each chain's exact inter energy loops only over its receptor-atom neighbour list."""
+        N = cur.shape[0]
+        if N == 0:
+            return
+        for x in (cur, cur_e, best, best_e):
+            assert x.is_contiguous() and x.dtype == torch.float32 and x.device.type == "cuda"
+        if exact:
+            assert self.c_rec.RN > 0, "exact mode needs receptor atoms (Problem.rec)"
+        cl, ci = self._i32(chain_lig), self._i32(chain_id)
+        if order is None:
+            order = self.chain_order(cl)
+        a = _lib.McArgs()
+        a.chain_lig, a.chain_id, a.n_chains = _lib.ptr(cl), _lib.ptr(ci), N
+        keep = [cl, ci, order]
+        if nbr is not None:
+            nbr, nbr_n = self._i32(nbr), self._i32(nbr_n)
+            keep += [nbr, nbr_n]
+            a.nbr, a.nbr_n, a.nb_max = _lib.ptr(nbr), _lib.ptr(nbr_n), int(nbr.shape[1])
+        else:
+            a.nbr = a.nbr_n = None
+            a.nb_max = 0
+        a.cur, a.cur_e, a.best, a.best_e = _lib.ptr(cur), _lib.ptr(cur_e), _lib.ptr(best), _lib.ptr(best_e)
+        a.init_opt, a.mc_steps, a.bfgs_iters = int(init_opt), int(mc_steps), int(bfgs_iters)
+        a.temp, a.amp_pos, a.amp_rot = float(temp), float(amp_pos), float(amp_rot)
+        a.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+        a.step_offset, a.exact = int(step_offset), int(exact)
+        a.order, a.queue, a.evals = _lib.ptr(order), _lib.ptr(self.queue), _lib.ptr(self.evals)
+        with torch.cuda.device(self.device):
+            _lib.call("adock_mc", self.c_lig, self.c_work, self.c_grids, self.c_sf, self.c_rec, a, _lib.stream_ptr())
+        self._keep_mc = keep
+
+    def stage_a(self, conf_h, quats, trans, ntrans, cap):
+        """conf_h [L, C, AM, 3] heavy-atom conformer coords (ligand frame), quats [Q, 4], trans [L, NT, 3],
+        ntrans [L] -> (best_e [L, C*Q], best_i [L, C*Q] index into trans)."""
+        L, C = conf_h.shape[:2]
+        Q, NT = quats.shape[0], trans.shape[1]
+        be = torch.empty(L * C * Q, device=self.device)
+        bi = torch.empty(L * C * Q, dtype=torch.int32, device=self.device)
+        keep = [conf_h.float().contiguous(), quats.float().contiguous(), trans.float().contiguous(),
+                self._i32(ntrans)]
+        with torch.cuda.device(self.device):
+            _lib.call("adock_stage_a", self.c_lig, self.c_work, self.c_grids, self.c_sf, _lib.ptr(keep[0]), C,
+                      _lib.ptr(keep[1]), Q, _lib.ptr(keep[2]), _lib.ptr(keep[3]), NT, float(cap), _lib.ptr(be),
+                      _lib.ptr(bi), _lib.stream_ptr())
+        return be.view(L, C * Q), bi.view(L, C * Q).long()
+
+    def receptor_neighbours(self, prob, chain_lig, states, K, margin):
+        """Per chain: indices of receptor atoms within cutoff + margin of any heavy atom of the chain's pose,
+        in receptor order (mckernel.py:662-688). Returns (nbr [N, NB] int32, nbr_n [N] int32)."""
+        assert self.c_rec.RN > 0, "neighbour lists need receptor atoms (Problem.rec)"
+        cut = float(prob.pot.p["cutoff"]) + margin
+        N = states.shape[0]
+        cl = self._i32(chain_lig)
+        st = states.to(self.device, torch.float32).contiguous()
+        cnt = torch.zeros(N, dtype=torch.int32, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.call("adock_neighbours", self.c_lig, self.c_work, self.c_sf, self.c_rec, _lib.ptr(cl), N, _lib.ptr(st),
+                      cut, None, _lib.ptr(cnt), 0, _lib.stream_ptr())
+            NB = max(1, int(cnt.max()) if N else 1)
+            nbr = torch.zeros(N, NB, dtype=torch.int32, device=self.device)
+            _lib.call("adock_neighbours", self.c_lig, self.c_work, self.c_sf, self.c_rec, _lib.ptr(cl), N, _lib.ptr(st),
+                      cut, _lib.ptr(nbr), _lib.ptr(cnt), NB, _lib.stream_ptr())
+        return nbr, cnt
+
+    def rescore64(self, chain_lig, states, exact=True):
+        """Float64 re-score on the device: (e_total [N] f64, e_intra [N] f64, X [N, AM, 3] f32 world coordinates).
+        exact=True uses pairwise inter energies over all receptor atoms (needs Problem.rec), else the grid."""
+        N = states.shape[0]
+        cl = self._i32(chain_lig)
+        st = states.to(self.device, torch.float32).contiguous()
+        et = torch.zeros(N, dtype=torch.float64, device=self.device)
+        ei = torch.zeros(N, dtype=torch.float64, device=self.device)
+        X = torch.zeros(N, self.AM, 3, device=self.device)
+        rec = self.c_rec if exact else _lib.Receptors()
+        if exact:
+            assert self.c_rec.RN > 0, "exact re-score needs receptor atoms (Problem.rec)"
+        with torch.cuda.device(self.device):
+            _lib.call("adock_rescore64", self.c_lig, self.c_work, self.c_grids, self.c_sf, rec, _lib.ptr(cl), N,
+                      _lib.ptr(st), _lib.ptr(et), _lib.ptr(ei), _lib.ptr(X), _lib.stream_ptr())
+        return et, ei, X
+
+
+# reference name, so callers that select the class by name find it
+KernelProblem = B200KernelProblem

@@ -1,0 +1,185 @@
+/*
+ * adock_b200 C-ABI: the docking hot path (receptor grid maps, batched pose energy/gradient, Monte-Carlo +
+ * BFGS search, rigid Stage-A enumeration, receptor neighbour lists) as hand-written sm_100a CUDA.
+ *
+ * Conventions
+ *  - Every entry point returns 0 on success or a negative ADOCK_E_* status; adock_last_error() returns a
+ *    thread-local message for the last failure on the calling thread.
+ *  - "dev" pointers are device memory of the current CUDA device; "host" pointers are small parameter tables
+ *    read during the call. Nothing here allocates device memory unless the comment says so; scratch space is
+ *    passed in by the caller (its size comes from the matching *_workspace query).
+ *  - `stream` is a cudaStream_t (NULL = legacy default stream). Calls are asynchronous on that stream;
+ *    device-side faults surface on the next synchronisation.
+ *  - Array layouts follow the reference's packing so its Python layer can bind these symbols directly
+ *    (state [N, 7+KM] = t(3), q(4, w x y z), theta(KM); gradient [N, 6+KM] = dE/dt(3), torque(3), dE/dtheta(KM)).
+ */
+#ifndef ADOCK_B200_H
+#define ADOCK_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ADOCK_ABI_VERSION 1
+
+#define ADOCK_OK 0
+#define ADOCK_E_ARG (-1)     /* bad argument: null pointer, bad size, limit exceeded */
+#define ADOCK_E_CUDA (-2)    /* CUDA runtime error (launch failure, bad device, ...) */
+#define ADOCK_E_DEVICE (-3)  /* device-side status word reported an error (see adock_last_error) */
+
+/* grid element storage */
+#define ADOCK_GRID_F32 0
+#define ADOCK_GRID_F16 1
+#define ADOCK_GRID_BF16 2
+
+/* ------------------------------------------------------------------------------------------------ tables */
+
+/* Scoring-function tables shared by all search calls (host struct, copied at each call). */
+typedef struct {
+    float prm[15];      /* g1_off, g1_w, g2_off, g2_w, rep_off, hyd_good, hyd_bad, hb_good, hb_bad, cutoff,
+                           w_g1, w_g2, w_rep, w_hyd, w_hb  (reference mckernel.py:594-596 order) */
+    int n_types;        /* entries used in the tables below (<= 64) */
+    float radius[64];
+    int hyd[64], don[64], acc[64];
+} adock_sf_t;
+
+/* Packed ligand batch (dev), reference pack_host layout (mckernel.py:547-599). */
+typedef struct {
+    const float* ref;          /* [L, AM, 3] ligand-frame heavy-atom coordinates */
+    const int* typ;            /* [L, AM] scoring type of each heavy atom */
+    const unsigned char* tm;   /* [L, KM, AM] torsion k moves atom a */
+    const int* ax;             /* [L, KM, 2] torsion axis atoms (parent side, child side) */
+    const float* axp;          /* [L, KM, 3] reference axis point */
+    const float* axu;          /* [L, KM, 3] reference axis unit vector */
+    const int* pr;             /* [L, P, 2] intra-ligand pairs */
+    const int* na;             /* [L] heavy atoms */
+    const int* nt;             /* [L] torsions */
+    const int* np;             /* [L] pairs */
+    const float* rg;           /* [L] radius of gyration */
+    const int* gslot;          /* [L, AM] grid slot of each atom */
+    const int* rec_idx;        /* [L] receptor of each ligand */
+    int L, AM, KM, P;
+} adock_ligands_t;
+
+/* Grid set (GridSet storage contract, grid.py:197-248), all dev. */
+typedef struct {
+    const void* flat;          /* concatenated per-receptor maps [T_r, nx, ny, nz], z fastest */
+    const long long* offs;     /* [R] element offset of each receptor's maps in flat */
+    const long long* dims;     /* [R, 3] */
+    const float* origin;       /* [R, 3] */
+    const float* lo;           /* [R, 3] box low corner (out-of-box penalty) */
+    const float* hi;           /* [R, 3] box high corner */
+    int R;
+    int dtype;                 /* ADOCK_GRID_* of flat */
+    float spacing, penalty;
+} adock_grids_t;
+
+/* Receptor atoms for the exact (grid-free) energy, dev; xyz == NULL when absent. */
+typedef struct {
+    const float* xyz;          /* [R, RN, 3] */
+    const int* typ;            /* [R, RN] */
+    const int* n;              /* [R] */
+    int RN;
+} adock_receptors_t;
+
+/* B200 working layout of a ligand batch, filled by adock_prepare (dev, caller-allocated). */
+typedef struct {
+    void* atoms;               /* [L, AM] float4: ref xyz + (gslot | typ << 16) bits */
+    void* masks;               /* [L, AM] uint32 torsion bitmask of each atom (KM <= 32) */
+    void* tors;                /* [L, KM, 2] float4: axp + ax0 bits, axu + ax1 bits */
+    void* pairs;               /* [L, P] int2: (i | j << 8 | flags << 16, radius-sum bits) */
+    void* info;                /* [L] int4: na, nt, np, rec_idx */
+    void* rg;                  /* [L] float */
+} adock_work_t;
+
+/* Monte-Carlo call arguments (reference run_mc, mckernel.py:706-726). */
+typedef struct {
+    const int* chain_lig;      /* dev [N] */
+    const int* chain_id;       /* dev [N] RNG stream id */
+    int n_chains;
+    const int* nbr;            /* dev [N, NB] receptor neighbour lists or NULL */
+    const int* nbr_n;          /* dev [N] */
+    int nb_max;
+    float* cur; float* cur_e; float* best; float* best_e;   /* dev, in place */
+    int init_opt, mc_steps, bfgs_iters;
+    float temp, amp_pos, amp_rot;
+    unsigned long long seed;
+    int step_offset;
+    int exact;
+    const int* order;          /* dev [N] processing order (longest first) or NULL */
+    int* queue;                /* dev, 1 int work counter, zeroed by the call on `stream` */
+    unsigned long long* evals; /* dev, 1 counter of energy evaluations (accumulated), or NULL */
+} adock_mc_args_t;
+
+/* ------------------------------------------------------------------------------------------------ misc */
+int adock_version(void);
+const char* adock_last_error(void);
+
+/* ------------------------------------------------------------------------------------------------ grids */
+
+/* Vina/Vinardo maps: replaces the reference build_grid kernel (grid.py:14-71, launched at grid.py:132-166).
+ * rec_xyz [n_rec,3], rec_types [n_rec] (dev); radius/hyd/don/acc [n_xs] and lig_types [n_lt] (host);
+ * prm[15] (host, grid.py:84-87 order: cutoff, g1_off, g1_w, g2_off, g2_w, rep_off, hyd_good, hyd_bad,
+ * hb_good, hb_bad, w_g1..w_hb). out (dev): [n_lt, nx, ny, nz], or [5, n_lt, nx, ny, nz] unweighted if per_term.
+ * n_lt <= 24 (grid.py:74 MAX_TYPES), n_xs <= 64. */
+int adock_grid_vina(const float* rec_xyz, const int* rec_types, int n_rec,
+                    const float* radius, const int* hyd, const int* don, const int* acc, int n_xs,
+                    const int* lig_types, int n_lt, float ox, float oy, float oz, float spacing,
+                    int nx, int ny, int nz, const float* prm, int per_term, float* out, void* stream);
+
+/* Fitted-function maps: replaces the reference build_grid_fit kernel (fit/gridfit.py:13-58, launched at
+ * gridfit.py:71-93). rec_xyz [n_rec,3], rec_ext [n_rec], rad_rec [n_rt] and W [n_rt, n_lt, 6] (dev);
+ * rad_lig [n_lt] and prm[12] (host, gridfit.py:80-81 order). out (dev) [n_lt, nx, ny, nz].
+ * n_lt <= 64 (gridfit.py:61 MAX_LT). */
+int adock_grid_fit(const float* rec_xyz, const int* rec_ext, int n_rec, const float* rad_rec, int n_rt,
+                   const float* rad_lig, int n_lt, const float* W, float ox, float oy, float oz, float spacing,
+                   int nx, int ny, int nz, const float* prm, float* out, void* stream);
+
+/* Down-convert FP32 maps to FP16 (dtype ADOCK_GRID_F16) or BF16 (ADOCK_GRID_BF16), round to nearest. */
+int adock_grid_convert(const float* src, void* dst, long long n, int dtype, void* stream);
+
+/* ------------------------------------------------------------------------------------------------ search */
+
+/* Fill the B200 working layout from the reference layout (once per problem). Scalar KM <= 32, AM <= 128. */
+int adock_prepare(const adock_ligands_t* lig, const adock_sf_t* sf, adock_work_t* work, void* stream);
+
+/* Energy + analytic pose gradient of N states: replaces eg_kernel (mckernel.py:411-447) /
+ * KernelProblem.energy_grad (mckernel.py:652-660). state [N, 7+KM], e [N], g [N, 6+KM] (dev). */
+int adock_eg(const adock_ligands_t* lig, const adock_work_t* work, const adock_grids_t* grids,
+             const adock_sf_t* sf, const adock_receptors_t* rec, const int* chain_lig, int n, const float* state,
+             float* e_out, float* g_out, int exact, void* stream);
+
+/* Monte Carlo + BFGS chains in place: replaces mc_kernel (mckernel.py:328-408) / KernelProblem.run_mc
+ * (mckernel.py:706-726). One persistent launch; chains are taken from a device work queue. */
+int adock_mc(const adock_ligands_t* lig, const adock_work_t* work, const adock_grids_t* grids,
+             const adock_sf_t* sf, const adock_receptors_t* rec, const adock_mc_args_t* mc, void* stream);
+
+/* Stage-A rigid enumeration: replaces stagea_kernel (mckernel.py:451-521) / KernelProblem.stage_a
+ * (mckernel.py:690-704). conf [L, C, AM, 3], quats [Q, 4], trans [L, NT, 3], ntrans [L] (dev);
+ * best_e, best_i [L, C*Q] (dev). */
+int adock_stage_a(const adock_ligands_t* lig, const adock_work_t* work, const adock_grids_t* grids,
+                  const adock_sf_t* sf, const float* conf, int C, const float* quats, int Q, const float* trans,
+                  const int* ntrans, int nt_max, float cap, float* best_e, int* best_i, void* stream);
+
+/* Receptor neighbour lists: replaces KernelProblem.receptor_neighbours (mckernel.py:662-688).
+ * Pass 1 (nbr == NULL): counts [N] of receptor atoms within `cut` of any heavy atom of each chain's pose.
+ * Pass 2: nbr [N, nb_max] filled in receptor index order (counts recomputed into nbr_n). */
+int adock_neighbours(const adock_ligands_t* lig, const adock_work_t* work, const adock_sf_t* sf,
+                     const adock_receptors_t* rec, const int* chain_lig, int n, const float* state, float cut,
+                     int* nbr, int* nbr_n, int nb_max, void* stream);
+
+/* Final re-score in float64 on the device: exact inter (pairwise over all receptor atoms when rec->xyz is
+ * set, else the grid), out-of-box penalty and intra energy of N states; writes e_total, e_intra [N] (dev,
+ * double) and world coordinates X [N, AM, 3] (dev, float). Replaces the rescoring half of finalize_kernel
+ * (search.py:506-537). */
+int adock_rescore64(const adock_ligands_t* lig, const adock_work_t* work, const adock_grids_t* grids,
+                    const adock_sf_t* sf, const adock_receptors_t* rec, const int* chain_lig, int n,
+                    const float* state, double* e_total, double* e_intra, float* X, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
