@@ -68,6 +68,9 @@ EXPORTS = tuple(_SIGS)
 
 _lib = None
 _lock = threading.Lock()
+# kernel launches issued through call() (each launching entry point issues one kernel)
+LAUNCHES = [0]
+_NO_LAUNCH = {"adock_version", "adock_last_error"}
 
 
 def load():
@@ -90,6 +93,8 @@ def call(name, *args):
     """Call an entry point; a non-zero status raises RuntimeError with the library's message."""
     lib = load()
     rc = getattr(lib, name)(*args)
+    if name not in _NO_LAUNCH and rc == 0:
+        LAUNCHES[0] += 1
     if rc != 0:
         msg = lib.adock_last_error().decode(errors="replace")
         raise RuntimeError(f"{name} failed ({rc}): {msg}")

@@ -301,7 +301,7 @@ __device__ float eval_eg(float* ws, const WSLayout& L, const float* s, float* g,
                     float rx = X0 - c.rx[3 * b], ry = X1 - c.rx[3 * b + 1], rz = X2 - c.rx[3 * b + 2];
                     float r2 = rx * rx + ry * ry + rz * rz;
                     if (r2 >= cut2) continue;
-                    const int tb = c.rt[b] & 63;   // type tables hold 64 entries (checked on the host)
+                    const int tb = c.rt[b] & 63;   // index kept inside the 64-entry type tables
                     const int fb = tt.flags[tb];
                     float r = sqrtf(r2), de;
                     ea += pair_energy(r, ra + tt.radius[tb], hyd_pair(fa, fb) | hb_pair(fa, fb), P.pp, de);
@@ -533,6 +533,7 @@ __global__ void __launch_bounds__(128) mc_kernel(const __grid_constant__ SearchP
     float* ws = (float*)smem4 + (size_t)wid * L.total;
     const int SDM = 7 + P.KM;
     unsigned n_eval = 0;
+    unsigned long long n_atom_eval = 0;
     while (true) {
         int idx = 0;
         if (lane == 0) idx = atomicAdd(M.queue, 1);
@@ -541,6 +542,7 @@ __global__ void __launch_bounds__(128) mc_kernel(const __grid_constant__ SearchP
         const int ch = M.order ? M.order[idx] : idx;
         const int l = M.chain_lig[ch];
         const int cid = M.chain_id[ch];
+        const unsigned n_eval_start = n_eval;
         Chain<APL> c;
         const int* nb = M.nbr ? M.nbr + (long long)ch * M.nb_max : nullptr;
         const int nbn = M.nbr ? M.nbr_n[ch] : 0;
@@ -604,9 +606,13 @@ __global__ void __launch_bounds__(128) mc_kernel(const __grid_constant__ SearchP
             M.cur_e[ch] = ec;
             M.best_e[ch] = eb;
         }
+        n_atom_eval += (unsigned long long)(n_eval - n_eval_start) * c.na;
         __syncwarp();
     }
-    if (M.evals && lane == 0 && n_eval) atomicAdd(M.evals, (unsigned long long)n_eval);
+    if (M.evals && lane == 0 && n_eval) {
+        atomicAdd(&M.evals[0], (unsigned long long)n_eval);
+        atomicAdd(&M.evals[1], n_atom_eval);
+    }
 }
 
 template <int APL, typename GT>

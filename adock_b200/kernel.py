@@ -36,6 +36,7 @@ class B200KernelProblem:
         self.t_lig = [T(ref), T(typ), T(tm), T(ax), T(axp), T(axu), T(pr), T(na), T(nt), T(npairs), T(rg), T(gsl),
                       prob.rec_idx.to(device=dev, dtype=torch.int32).contiguous()]
         self.na_host, self.nt_host = na.copy(), nt.copy()
+        self.h2d_bytes = int(sum(t.numel() * t.element_size() for t in self.t_lig[:12]))
         lt = _lib.Ligands()
         for name, t in zip(("ref", "typ", "tm", "ax", "axp", "axu", "pr", "na", "nt", "np", "rg", "gslot", "rec_idx"),
                            self.t_lig):
@@ -83,7 +84,7 @@ class B200KernelProblem:
         w.atoms, w.masks, w.tors, w.pairs, w.info, w.rg = [_lib.ptr(t) for t in self.t_work]
         self.c_work = w
         self.queue = torch.zeros(1, dtype=torch.int32, device=dev)
-        self.evals = torch.zeros(1, dtype=torch.int64, device=dev)
+        self.evals = torch.zeros(2, dtype=torch.int64, device=dev)  # energy evaluations, atom evaluations
         with torch.cuda.device(dev):
             _lib.call("adock_prepare", self.c_lig, self.c_sf, self.c_work, _lib.stream_ptr())
         self.L, self.SD, self.DM = L, 7 + KM, 6 + KM

@@ -1,0 +1,360 @@
+"""Benchmark: ligands docked per second on the batched uneven search workload.
+
+Workload (one step): 256 synthetic ligands (10-60 heavy atoms, 0-15 rotatable bonds, seeds 0-255 on rank 0)
+docked against the 1,500-atom synthetic receptor (22.5 A box, 61^3 x 8 Vina maps, FP32) with 32 MC chains x
+2,000 MC steps each (BFGS local optimisation, Vina iteration rule), BFGS refinement, exact polish of the top 32
+chains and finalize (top 9 poses). Ranks shard ligands (rank r docks seeds 256r .. 256r+255); no collective on
+the data path (weak scaling).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0). ``value`` times the search on device-resident inputs (maps, packed ligands);
+``e2e`` times the public ``dock_screen`` call from host arrays (map build, packing, host<->device copies,
+search, results back on the host). ``--impl reference`` times the reference's own CPU kernels (oracle/_ref, the
+reference's g++/OpenMP build) driven by the same search driver on the host cores, on a 4-ligand sample.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_LIGANDS = 256
+CHAINS = 32
+MC_STEPS = 2000
+METRIC = "ligands docked/s (plain FP32 search: 32 MC chains x 2000 steps + BFGS, top-9 poses)"
+UNIT = "ligands/s"
+WORKLOAD = ("batched uneven search: 256 synthetic ligands (10-60 heavy atoms, 0-15 torsions) x 32 chains x 2000 "
+            "MC steps vs 1500-atom receptor, 61^3 x 8 Vina maps (FP32)")
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ligands", type=int, default=N_LIGANDS)
+    ap.add_argument("--mc-steps", type=int, default=MC_STEPS)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def _workload(rank, n_lig, mc_steps):
+    from adock_b200 import params, synth
+    rec = synth.config_receptor(0)
+    ligs = synth.ligand_set(n_lig, (10, 60), (0, 15), seed0=rank * n_lig)
+    cfg = params.workload_preset(CHAINS, mc_steps)
+    return rec, ligs, cfg
+
+
+def _cpu_sample(ligs):
+    """4 ligands at the 1/8, 3/8, 5/8, 7/8 quantiles of the heavy-atom count (a size-representative sample)."""
+    order = sorted(range(len(ligs)), key=lambda i: (ligs[i].n, i))
+    pick = [order[int(len(order) * f)] for f in (0.125, 0.375, 0.625, 0.875)]
+    return [ligs[i] for i in pick]
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of SM clock and throttle reasons during the timed region."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.rows, self.proc = [], None
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(gpu_index)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            p = [x.strip() for x in line.split(",")]
+            if len(p) == 7:
+                self.rows.append(p)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm, mx, reasons = [], None, set()
+        for r in self.rows:
+            try:
+                sm.append(float(r[0]))
+                mx = float(r[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, r[3:]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        load = [s for s in sm if mx and s > 0.3 * mx] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _traffic_per_atom_eval():
+    """DRAM bytes per atom evaluation of the MC kernel from the committed ncu summary (None if absent)."""
+    f = ROOT / "profiles" / "mc_kernel_traffic.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("dram_bytes_per_atom_eval:"):
+            return float(line.split(":")[1])
+    return None
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the reference's CPU kernels (oracle/_ref) on the host cores, 4-ligand sample per step."""
+    if rank != 0:
+        return None
+    import torch
+    from oracle import ref as R
+    from adock_b200 import params
+    from adock_b200.grid import GridSet, grid_dims
+    from adock_b200.ligand import LigandBatch
+    from adock_b200.problem import PairPotential, Problem, pad_receptors
+    from adock_b200.search import dock_problem_kernel
+    import numpy as np
+    if not R.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref (the reference's CPU build) was not built on this tree"}
+    threads = R.threads()
+    torch.set_num_threads(threads)
+    rec, ligs, cfg = _workload(0, args.ligands, args.mc_steps)
+    sample = _cpu_sample(ligs)
+    prob = _cpu_problem(rec, sample)
+    times = []
+    for it in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        dock_problem_kernel(prob, prob._bc, prob._bs, cfg, seed=0, kernel_factory=R.RefKernelProblem)
+        dt = time.perf_counter() - t0
+        if it >= args.warmup:
+            times.append(dt)
+    v = len(sample) * len(times) / sum(times)
+    sample_desc = (f"{len(sample)} ligands of the workload (heavy atoms {[p.n for p in sample]}) x {CHAINS} chains x "
+                   f"{args.mc_steps} steps, full search per step")
+    return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": WORKLOAD, "ligands_per_step": len(sample), "chains": CHAINS, "mc_steps": args.mc_steps,
+                       "parallelism": "host cores (OpenMP)"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample_desc},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def _cpu_problem(rec, ligs):
+    """Problem on the host for the CPU baselines: maps from the reference CPU builder."""
+    import numpy as np
+    import torch
+    from oracle import ref as R
+    from adock_b200 import params
+    from adock_b200.grid import GridSet, grid_dims
+    from adock_b200.ligand import LigandBatch
+    from adock_b200.problem import PairPotential, Problem, pad_receptors
+    sfp = params.sf_params("vina")
+    lt = np.unique(np.concatenate([[0]] + [l.types for l in ligs]))
+    c, s = rec["center"], rec["size"]
+    o = c - s / 2
+    G = R.build_grid(rec["rec_xyz"], rec["rec_types"], sfp, o, params.GRID_SPACING, grid_dims(s, params.GRID_SPACING), lt)
+    slot = -np.ones((1, params.N_XS), np.int64)
+    slot[0, lt] = np.arange(len(lt))
+    f = lambda a: torch.tensor(np.asarray(a, np.float32)[None])
+    gs = GridSet([torch.as_tensor(G)], f(o), f(o), f(c + s / 2), params.GRID_SPACING, params.OUT_OF_BOX_PENALTY,
+                 slot=torch.as_tensor(slot), n_types=params.N_XS)
+    lb = LigandBatch(ligs, "cpu")
+    prob = Problem(gs, lb, torch.zeros(len(ligs), dtype=torch.long), PairPotential(sfp), rec=pad_receptors([rec], "cpu"))
+    prob._bc = torch.tensor(c, dtype=torch.float32)[None].expand(len(ligs), 3)
+    prob._bs = [s] * len(ligs)
+    return prob
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from adock_b200 import _lib, params
+    from adock_b200.grid import make_gridset
+    from adock_b200.kernel import B200KernelProblem
+    from adock_b200.ligand import LigandBatch
+    from adock_b200.problem import PairPotential, Problem, pad_receptors
+    from adock_b200.screen import dock_screen
+    from adock_b200.search import dock_problem_kernel
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    rec, ligs, cfg = _workload(rank, args.ligands, args.mc_steps)
+    sfp = params.sf_params("vina")
+    box = {"center": rec["center"], "size": rec["size"]}
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    # ---- device-resident inputs (built before the timed region) ----
+    types = np.unique(np.concatenate([l.types for l in ligs]))
+    gs = make_gridset([rec], sfp, params.GRID_SPACING, params.OUT_OF_BOX_PENALTY, device=dev, lig_types=[types])
+    lb = LigandBatch(ligs, dev)
+    prob = Problem(gs, lb, torch.zeros(len(ligs), dtype=torch.long, device=dev), PairPotential(sfp, dev),
+                   rec=pad_receptors([rec], dev))
+    kp = B200KernelProblem(prob)
+    bc = torch.tensor(rec["center"], dtype=torch.float32, device=dev)[None].expand(len(ligs), 3)
+    bs = [rec["size"]] * len(ligs)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # > 126 MB L2
+
+    def step(stats):
+        kp.evals.zero_()
+        dock_problem_kernel(prob, bc, bs, cfg, seed=0, stats=stats, kernel_factory=lambda p: kp)
+
+    for _ in range(args.warmup):
+        step({})
+    barrier()
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    clocks = ClockSampler(vis.split(",")[local_rank] if vis else local_rank)
+    launches0 = _lib.LAUNCHES[0]
+    step_ms, mc_ms, evals, atom_evals = [], [], 0, 0
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        st = {}
+        e0.record()
+        step(st)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        step_ms.append(e0.elapsed_time(e1))
+        mc_ms.append(st["mc_ms"])
+        evals += st["evals"]
+        atom_evals += st["atom_evals"]
+    barrier()
+    clk = clocks.stop()
+    launches = _lib.LAUNCHES[0] - launches0
+    t_rank = sum(step_ms)
+    t_max = t_rank
+    if world > 1:
+        tt = torch.tensor([t_rank], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt)
+    value = args.ligands * world * args.steps / (t_max / 1e3)
+
+    # ---- end to end through the public API from host arrays ----
+    e2e = None
+    if not args.no_e2e:
+        st = {}
+        dock_screen(rec, box, ligs, cfg, device=dev, stats=st)   # warm-up (allocator, module load)
+        barrier()
+        e2e_ms, h2d, d2h = [], 0, 0
+        for _ in range(max(1, min(args.steps, 3))):
+            flush.zero_()
+            st = {}
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            res = dock_screen(rec, box, ligs, cfg, device=dev, stats=st)
+            e1.record()
+            torch.cuda.synchronize(dev)
+            e2e_ms.append(e0.elapsed_time(e1))
+            h2d, d2h = st.get("h2d_bytes", 0), st.get("d2h_bytes", 0)
+            assert len(res) == len(ligs) and all(len(r["affinity"]) >= 1 for r in res)
+        t = sum(e2e_ms)
+        if world > 1:
+            tt = torch.tensor([t], device=dev, dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt)
+        e2e = {"value": args.ligands * world * len(e2e_ms) / (t / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h)}
+
+    # ---- roofline of the dominant kernel (MC + BFGS persistent kernel) ----
+    peak, peak_kind = _peaks()
+    mc_s = sum(mc_ms) / 1e3
+    alg_bytes = atom_evals * 8 * 4           # 8 FP32 corner values gathered per atom evaluation
+    achieved = alg_bytes / mc_s / 1e9
+    tpa = _traffic_per_atom_eval()
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": peak_kind, "kernel": "mc_kernel",
+            "traffic": (tpa * atom_evals / args.steps) if tpa is not None else None,
+            "algorithmic_bytes_per_launch": alg_bytes / args.steps, "launch_ms": 1e3 * mc_s / args.steps}
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, shapes of the batched uneven workload)",
+           "config": {"workload": WORKLOAD, "ligands_per_gpu": args.ligands, "chains": CHAINS, "mc_steps": args.mc_steps,
+                      "l2": "flushed (256 MB write) between timed steps", "parallelism": f"ligand shards x{world}"},
+           "evals_per_s": evals * world / mc_s, "mc_share_of_step": sum(mc_ms) / sum(step_ms),
+           "roofline": roof, "clocks": clk, "gpu_launches": launches, "e2e": e2e}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = _cpu_baseline(ligs, rec, cfg)
+    return out
+
+
+def _cpu_baseline(ligs, rec, cfg):
+    """The reference CPU kernels (or the oracle's restatement where oracle/_ref is absent) on a 4-ligand sample."""
+    import torch
+    from oracle import port
+    from oracle import ref as R
+    from adock_b200.search import dock_problem_kernel
+    sample = _cpu_sample(ligs)
+    threads = R.threads()
+    torch.set_num_threads(threads)
+    prob = _cpu_problem(rec, sample) if R.available() else None
+    kind = "reference" if R.available() else "port"
+    if prob is None:
+        return {"value": None, "unit": UNIT, "cores": threads, "kind": kind, "sample": "oracle/_ref not built"}
+    factory = R.RefKernelProblem if kind == "reference" else (lambda p: R.RefKernelProblem(p, port.PortProblem))
+    t0 = time.perf_counter()
+    dock_problem_kernel(prob, prob._bc, prob._bs, cfg, seed=0, kernel_factory=factory)
+    dt = time.perf_counter() - t0
+    return {"value": len(sample) / dt, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"{len(sample)} ligands (heavy atoms {[p.n for p in sample]}) x {CHAINS} chains x "
+                      f"{cfg['mc_steps']} steps, one full search, {dt:.1f} s"}
+
+
+def main():
+    args = _args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        if args.impl == "ours":
+            torch.cuda.set_device(local_rank)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+    else:
+        out = run_ours(args, rank, world, local_rank)
+    if rank == 0 and out is not None:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -111,7 +111,7 @@ typedef struct {
     int exact;
     const int* order;          /* dev [N] processing order (longest first) or NULL */
     int* queue;                /* dev, 1 int work counter, zeroed by the call on `stream` */
-    unsigned long long* evals; /* dev, 1 counter of energy evaluations (accumulated), or NULL */
+    unsigned long long* evals; /* dev, 2 counters (accumulated): energy evaluations, atom evaluations; or NULL */
 } adock_mc_args_t;
 
 /* ------------------------------------------------------------------------------------------------ misc */

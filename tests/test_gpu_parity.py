@@ -216,7 +216,7 @@ def test_neighbours_match_torch(dev):
                     torch.as_tensor(st[i:i + 1, 7:7 + pc.lb.K]))
         sub = pc.lb.subset(torch.tensor([l]))
         X = pose_coords(sub, t[None], q[None], torch.zeros_like(t)[None], th[None])[0, 0].numpy()
-        X = X[pc.lb.preps[l].heavy]
+        X = X[:pc.lb.preps[l].n][pc.lb.preps[l].heavy]
         d = np.linalg.norm(X[:, None] - rx[None], axis=-1).min(0)
         want = np.where(d < cut)[0]
         border = np.abs(d - cut) < 1e-4
