@@ -63,6 +63,8 @@ _SIGS = {
     "adock_stage_a": ([SP(Ligands), SP(Work), SP(Grids), SP(SF), P, I, P, I, P, P, I, F, P, P, P], I),
     "adock_neighbours": ([SP(Ligands), SP(Work), SP(SF), SP(Receptors), P, I, P, F, P, P, I, P], I),
     "adock_rescore64": ([SP(Ligands), SP(Work), SP(Grids), SP(SF), SP(Receptors), P, I, P, P, P, P, P], I),
+    "adock_mc_noalloc_scratch_bytes": ([I, I, I, I], ctypes.c_size_t),
+    "adock_mc_noalloc": ([SP(Ligands), SP(Grids), SP(SF), SP(Receptors), SP(McArgs), P], I),
 }
 EXPORTS = tuple(_SIGS)
 
@@ -70,7 +72,7 @@ _lib = None
 _lock = threading.Lock()
 # kernel launches issued through call() (each launching entry point issues one kernel)
 LAUNCHES = [0]
-_NO_LAUNCH = {"adock_version", "adock_last_error"}
+_NO_LAUNCH = {"adock_version", "adock_last_error", "adock_mc_noalloc_scratch_bytes"}
 
 
 def load():

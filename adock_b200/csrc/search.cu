@@ -1186,3 +1186,75 @@ extern "C" int adock_rescore64(const adock_ligands_t* lig, const adock_work_t* w
     ADOCK_CUDA(cudaGetLastError());
     return ADOCK_OK;
 }
+
+// ------------------------------------------------------------------------------------------ no-allocation MC
+// Some callers cannot allocate device memory: code that runs while a CUDA stream is being captured into a graph
+// by a framework that forbids allocations during capture, embedders whose memory pool owns every device byte, or
+// callers that only receive raw input/output pointers from a host application. adock_mc needs caller-allocated
+// scratch (the B200 working layout of the ligand batch and a one-word work-queue counter); this variant keeps that
+// scratch in one fixed-size device array instead, so the caller passes only inputs and outputs.
+//
+// The array lives for the whole process on every device that loads the library. In host code its name is only
+// a host-side stand-in; the device address comes from cudaGetSymbolAddress, taken once per device on the first
+// call with that device current (so the first call on a device should come before any stream capture). Every
+// call reuses the same array: the work counter is cleared by each call, the working layout is rewritten by each
+// call, and calls that overlap on the GPU (different streams, or other threads) race on it.
+#define ADOCK_NOALLOC_SCRATCH_BYTES ADOCK_NOALLOC_SCRATCH_MAX
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[ADOCK_NOALLOC_SCRATCH_BYTES];
+
+namespace adock {
+static void* g_noalloc_ptr[64];
+static int g_noalloc_ready[64];
+
+static size_t round256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static int noalloc_scratch(void** out) {
+    int dev = 0;
+    ADOCK_CUDA(cudaGetDevice(&dev));
+    ADOCK_CHECK_ARG(dev >= 0 && dev < 64, "device index %d out of range", dev);
+    if (!__atomic_load_n(&g_noalloc_ready[dev], __ATOMIC_ACQUIRE)) {
+        void* p = nullptr;
+        ADOCK_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_ptr[dev] = p;
+        __atomic_store_n(&g_noalloc_ready[dev], 1, __ATOMIC_RELEASE);
+    }
+    *out = g_noalloc_ptr[dev];
+    return ADOCK_OK;
+}
+}  // namespace adock
+
+extern "C" size_t adock_mc_noalloc_scratch_bytes(int L, int AM, int KM, int P) {
+    using adock::round256;
+    return round256(sizeof(int)) + round256((size_t)L * AM * 16) + round256((size_t)L * AM * 4) +
+           round256((size_t)L * KM * 32) + round256((size_t)L * P * 8) + round256((size_t)L * 16) +
+           round256((size_t)L * 4);
+}
+
+extern "C" int adock_mc_noalloc(const adock_ligands_t* lig, const adock_grids_t* grids, const adock_sf_t* sf,
+                                const adock_receptors_t* rec, const adock_mc_args_t* mc, void* stream) {
+    ADOCK_CHECK_ARG(lig && grids && sf && mc, "null argument");
+    ADOCK_CHECK_ARG(lig->L >= 1 && lig->AM >= 32 && lig->KM >= 1 && lig->P >= 1, "bad ligand batch dimensions");
+    const size_t need = adock_mc_noalloc_scratch_bytes(lig->L, lig->AM, lig->KM, lig->P);
+    ADOCK_CHECK_ARG(need <= ADOCK_NOALLOC_SCRATCH_BYTES,
+                    "batch needs %zu bytes of scratch; adock_mc_noalloc holds at most %u (use adock_mc)", need,
+                    (unsigned)ADOCK_NOALLOC_SCRATCH_BYTES);
+    void* base = nullptr;
+    int rc = noalloc_scratch(&base);
+    if (rc) return rc;
+    unsigned char* p = (unsigned char*)base;
+    int* queue = (int*)p;
+    p += round256(sizeof(int));
+    adock_work_t work;
+    work.atoms = p; p += round256((size_t)lig->L * lig->AM * 16);
+    work.masks = p; p += round256((size_t)lig->L * lig->AM * 4);
+    work.tors = p;  p += round256((size_t)lig->L * lig->KM * 32);
+    work.pairs = p; p += round256((size_t)lig->L * lig->P * 8);
+    work.info = p;  p += round256((size_t)lig->L * 16);
+    work.rg = p;
+    rc = adock_prepare(lig, sf, &work, stream);
+    if (rc) return rc;
+    adock_mc_args_t m = *mc;
+    m.queue = queue;   // adock_mc clears the counter on `stream` before its launch
+    return adock_mc(lig, &work, grids, sf, rec, &m, stream);
+}

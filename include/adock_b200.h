@@ -179,6 +179,22 @@ int adock_rescore64(const adock_ligands_t* lig, const adock_work_t* work, const 
                     const adock_sf_t* sf, const adock_receptors_t* rec, const int* chain_lig, int n,
                     const float* state, double* e_total, double* e_intra, float* X, void* stream);
 
+/* ------------------------------------------------------------------------------------------------ no allocation */
+
+/* No counterpart in the reference. adock_mc for callers that cannot allocate device memory (a stream being
+ * captured into a graph by a framework that forbids allocation during capture, a memory pool that owns the
+ * device, a host application that passes only raw input/output pointers). The ligand working layout and the
+ * work-queue counter that adock_mc takes from the caller live instead in one library-owned device array of
+ * ADOCK_NOALLOC_SCRATCH_MAX bytes, held on every device that loads the library until the process exits.
+ * Inputs and outputs are as for adock_mc (mc->queue is ignored; mc->order and mc->evals are optional). Batches
+ * whose scratch (adock_mc_noalloc_scratch_bytes) exceeds the limit are rejected with ADOCK_E_ARG. No call
+ * allocates. The first call on a device looks up the array's device address and should come before any stream
+ * capture on that device. All calls share the array: calls that overlap on the GPU race. */
+#define ADOCK_NOALLOC_SCRATCH_MAX (16u << 20)
+size_t adock_mc_noalloc_scratch_bytes(int L, int AM, int KM, int P);
+int adock_mc_noalloc(const adock_ligands_t* lig, const adock_grids_t* grids, const adock_sf_t* sf,
+                     const adock_receptors_t* rec, const adock_mc_args_t* mc, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
