@@ -47,7 +47,7 @@ class McArgs(ctypes.Structure):
     _fields_ = [("chain_lig", P), ("chain_id", P), ("n_chains", I), ("nbr", P), ("nbr_n", P), ("nb_max", I),
                 ("cur", P), ("cur_e", P), ("best", P), ("best_e", P), ("init_opt", I), ("mc_steps", I),
                 ("bfgs_iters", I), ("temp", F), ("amp_pos", F), ("amp_rot", F), ("seed", ctypes.c_ulonglong),
-                ("step_offset", I), ("exact", I), ("order", P), ("queue", P), ("evals", P)]
+                ("step_offset", I), ("exact", I), ("order", P), ("queue", P), ("evals", P), ("variant", I)]
 
 
 SP = ctypes.POINTER

@@ -1,0 +1,82 @@
+"""Autotuner for the persistent Monte-Carlo kernel's launch shape.
+
+The MC kernel trades registers per thread for resident warps per SM (``adock_mc_args_t.variant``: 4, 6 or 8
+resident 128-thread blocks per SM, i.e. 128, 80 or 64 registers). Which is fastest depends on the atom bucket
+(AM), the torsion bucket (KM), the map storage type and the GPU. ``tune_mc`` times one MC step of a sample of the
+batch's chains (most expensive ligands included) under each variant and keeps the fastest; results are cached per
+(device name, AM, KM, map dtype) for the life of the process and in ``$ADOCK_TUNE_CACHE`` (a JSON file) if set.
+"""
+from __future__ import annotations
+
+import json
+import os
+import threading
+
+import torch
+
+VARIANTS = (1, 2, 3)
+_cache = {}
+_lock = threading.Lock()
+
+
+def _key(kp):
+    return f"{torch.cuda.get_device_name(kp.device)}|AM{kp.AM}|KM{kp.KM}|{kp.grid_dtype}"
+
+
+def _load_file():
+    path = os.environ.get("ADOCK_TUNE_CACHE")
+    if path and os.path.exists(path):
+        try:
+            with open(path) as fh:
+                _cache.update(json.load(fh))
+        except (OSError, ValueError):
+            pass
+
+
+def _save_file():
+    path = os.environ.get("ADOCK_TUNE_CACHE")
+    if path:
+        tmp = f"{path}.{os.getpid()}.tmp"
+        with open(tmp, "w") as fh:
+            json.dump(_cache, fh, indent=1)
+        os.replace(tmp, path)
+
+
+def tune_mc(kp, chain_lig, state, max_chains=4096, steps=1):
+    """Return the fastest MC launch variant for this kernel object (cached)."""
+    key = _key(kp)
+    with _lock:
+        if not _cache:
+            _load_file()
+        if key in _cache:
+            return int(_cache[key]["variant"])
+    dev = kp.device
+    N = state.shape[0]
+    order = kp.chain_order(chain_lig).long()
+    # the most expensive chains plus an even spread of the rest (the tail of the persistent launch matters)
+    take = order[: max_chains // 4].tolist() + order[max_chains // 4:: max(1, N // max_chains)].tolist()
+    idx = torch.tensor(sorted(set(take))[:max_chains], device=dev, dtype=torch.long)
+    cl = chain_lig[idx].to(torch.int32)
+    ci = torch.arange(len(idx), device=dev, dtype=torch.int32)
+    times = {}
+    for v in VARIANTS:
+        cur = state[idx].contiguous().clone()
+        best = cur.clone()
+        ce = torch.zeros(len(idx), device=dev)
+        be = torch.full((len(idx),), float("inf"), device=dev)
+        kp.run_mc(cl, ci, cur, ce, best, be, False, 1, 3, 1.2, 2.0, 2.0, 1, 0, variant=v)   # warm-up / load
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        kp.run_mc(cl, ci, cur, ce, best, be, False, steps, 0, 1.2, 2.0, 2.0, 1, 0, variant=v)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        times[v] = e0.elapsed_time(e1)
+    best_v = min(times, key=times.get)
+    with _lock:
+        _cache[key] = {"variant": best_v, "ms": {str(k): round(t, 3) for k, t in times.items()}, "chains": len(idx)}
+        _save_file()
+    return best_v
+
+
+def cached():
+    return dict(_cache)

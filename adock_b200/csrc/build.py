@@ -12,15 +12,16 @@ HERE = Path(__file__).resolve().parent
 PKG = HERE.parent
 ROOT = PKG.parent
 LIB = PKG / "libadock_b200.so"
-SOURCES = ["abi.cu", "grid.cu", "search.cu"]
+SOURCES = ["abi.cu", "grid.cu", "search.cu", "search_f32.cu", "search_f16.cu", "search_bf16.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-Xcompiler", "-fPIC",
-         "-shared", "-cudart", "shared", "-I", str(ROOT / "include")]
+         "-I", str(ROOT / "include")]
+LINK = ["-shared", "-cudart", "shared"]
 
 
 def _digest():
     h = hashlib.sha1()
-    for f in SOURCES + ["common.cuh"]:
+    for f in SOURCES + ["common.cuh", "search_impl.cuh"]:
         h.update((HERE / f).read_bytes())
     h.update((ROOT / "include" / "adock_b200.h").read_bytes())
     h.update(" ".join(FLAGS).encode())
@@ -33,12 +34,22 @@ def build(force=False, verbose=False):
     if not force and LIB.exists() and stamp.exists() and stamp.read_text() == dg:
         return LIB
     tmp = LIB.with_name(LIB.name + f".{os.getpid()}.tmp")
-    cmd = [NVCC] + FLAGS + [str(HERE / s) for s in SOURCES] + ["-o", str(tmp)]
-    if verbose:
-        print(" ".join(cmd))
-    r = subprocess.run(cmd, capture_output=True, text=True)
+    objdir = ROOT / "_build"
+    objdir.mkdir(exist_ok=True)
+    objs = [objdir / (Path(s).stem + ".o") for s in SOURCES]
+    procs = []
+    for s, o in zip(SOURCES, objs):       # one nvcc per translation unit, in parallel
+        cmd = [NVCC] + FLAGS + ["-c", str(HERE / s), "-o", str(o)]
+        if verbose:
+            print(" ".join(cmd))
+        procs.append((s, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
+    for s, pr in procs:
+        _, err = pr.communicate()
+        if pr.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {s}:\n{err[-6000:]}")
+    r = subprocess.run([NVCC] + LINK + [str(o) for o in objs] + ["-o", str(tmp)], capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError(f"nvcc failed:\n{r.stderr[-6000:]}")
+        raise RuntimeError(f"nvcc link failed:\n{r.stderr[-6000:]}")
     os.replace(tmp, LIB)
     stamp.write_text(dg)
     return LIB

@@ -245,10 +245,12 @@ __global__ void __launch_bounds__(TILE_THREADS) grid_fit_kernel(const float* __r
 
 template <typename T>
 __global__ void convert_kernel(const float* __restrict__ src, T* __restrict__ dst, long long n);
+// FP16 saturates at +-65504 (map values inside receptor atoms can exceed the FP16 range; a clamped value keeps
+// such points repulsive instead of turning the interpolation into inf/NaN)
 template <>
 __global__ void convert_kernel<__half>(const float* __restrict__ src, __half* __restrict__ dst, long long n) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        dst[i] = __float2half_rn(src[i]);
+        dst[i] = __float2half_rn(fminf(fmaxf(src[i], -65504.f), 65504.f));
 }
 template <>
 __global__ void convert_kernel<__nv_bfloat16>(const float* __restrict__ src, __nv_bfloat16* __restrict__ dst, long long n) {

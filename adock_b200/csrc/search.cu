@@ -1,68 +1,29 @@
-// Search kernels of the docking hot path (sm_100a): working-layout preparation, batched energy + analytic pose
-// gradient, Vina-style BFGS, persistent Monte-Carlo chains, Stage-A rigid enumeration, receptor neighbour lists
-// and the float64 final re-score.
-//
-// Execution model: one warp owns one chain (pose). Lanes own heavy atoms a = lane + 32*i (i < APL, AM = 32*APL)
-// whose ligand-frame coordinates, grid slot and torsion bitmask stay in registers for the whole chain. Per-warp
-// shared memory holds world coordinates, force accumulators, torsion axes, the BFGS inverse Hessian and the
-// state vectors. The Monte-Carlo kernel is persistent: warps pull chains from a device work counter (longest
-// ligands first), so uneven ligands do not leave SMs idle at the tail.
-#include "common.cuh"
-#include <algorithm>
+// Search entry points of the docking hot path (sm_100a): working-layout preparation (with the intra-pair round
+// schedule), receptor neighbour lists, and the C-ABI of the energy/gradient, Monte-Carlo, Stage-A and float64
+// re-score kernels. The grid-dtype-templated kernels live in search_impl.cuh and are instantiated in
+// search_f32.cu / search_f16.cu / search_bf16.cu.
+#include "search_impl.cuh"
 #include <stdio.h>
 
 namespace adock {
 
-#define EPSF 1.1920929e-07f
+ADOCK_SEARCH_EXTERN(float)
+ADOCK_SEARCH_EXTERN(__half)
+ADOCK_SEARCH_EXTERN(__nv_bfloat16)
 
-struct SearchParams {
-    // B200 working layout
-    const float4* atoms;   // [L, AM]
-    const uint32_t* masks; // [L, AM]
-    const float4* tors;    // [L, KM, 2]
-    const int2* pairs;     // [L, P]
-    const int4* info;      // [L] na, nt, np, rec_idx
-    const float* rg;       // [L]
-    int AM, KM, P;
-    // grids
-    const void* flat;
-    const long long* offs;
-    const long long* dims;
-    const float* origin;
-    const float* lo;
-    const float* hi;
-    float inv_s, pen;
-    // receptor atoms for exact mode
-    const float* rxyz;
-    const int* rtyp;
-    const int* rn;
-    int RN;
-    PairPrm pp;
-    int n_types;
-};
-
-// type tables for exact mode, staged in shared memory by every block that may need them
-struct TypeTables {
-    float radius[64];
-    int flags[64];  // bit0 hydrophobic, bit1 donor, bit2 acceptor
-};
-
-__device__ __forceinline__ int hb_pair(int fa, int fb) {
-    return (((fa & 2) && (fb & 4)) || ((fa & 4) && (fb & 2))) ? PF_HB : 0;
-}
-__device__ __forceinline__ int hyd_pair(int fa, int fb) { return ((fa & 1) && (fb & 1)) ? PF_HYD : 0; }
+static inline int pad32(int x) { return ((x + 31) / 32) * 32; }
 
 // ------------------------------------------------------------------------------------------ prepare
 __global__ void prepare_kernel(adock_ligands_t lig, TypeTables tt, float4* atoms, uint32_t* masks, float4* tors,
-                               int2* pairs, int4* info, float* rg) {
+                               int4* info, float* rg) {
     const int l = blockIdx.x;
-    const int AM = lig.AM, KM = lig.KM, P = lig.P;
+    const int AM = lig.AM, KM = lig.KM;
     const int na = lig.na[l], nt = lig.nt[l], np = lig.np[l];
     for (int a = threadIdx.x; a < AM; a += blockDim.x) {
         const float* r = lig.ref + ((long long)l * AM + a) * 3;
-        int slot = lig.gslot[(long long)l * AM + a];
-        int typ = lig.typ[(long long)l * AM + a];
-        float4 v = make_float4(r[0], r[1], r[2], __int_as_float((slot & 0xffff) | (typ << 16)));
+        const int slot = lig.gslot[(long long)l * AM + a];
+        const int typ = lig.typ[(long long)l * AM + a];
+        const float4 v = make_float4(r[0], r[1], r[2], __int_as_float((slot & 0xffff) | (typ << 16)));
         uint32_t m = 0;
         if (a < na)
             for (int k = 0; k < nt && k < 32; ++k) m |= (lig.tm[((long long)l * KM + k) * AM + a] ? 1u : 0u) << k;
@@ -76,657 +37,71 @@ __global__ void prepare_kernel(adock_ligands_t lig, TypeTables tt, float4* atoms
         tors[((long long)l * KM + k) * 2] = make_float4(p[0], p[1], p[2], __int_as_float(x[0]));
         tors[((long long)l * KM + k) * 2 + 1] = make_float4(u[0], u[1], u[2], __int_as_float(x[1]));
     }
-    for (int q = threadIdx.x; q < P; q += blockDim.x) {
-        int i = lig.pr[((long long)l * P + q) * 2], j = lig.pr[((long long)l * P + q) * 2 + 1];
-        int ti = lig.typ[(long long)l * AM + i], tj = lig.typ[(long long)l * AM + j];
-        ti = ti < 0 ? 0 : ti;
-        tj = tj < 0 ? 0 : tj;
-        int fl = hyd_pair(tt.flags[ti], tt.flags[tj]) | hb_pair(tt.flags[ti], tt.flags[tj]);
-        float rs = tt.radius[ti] + tt.radius[tj];
-        pairs[(long long)l * P + q] = make_int2((i & 0xff) | ((j & 0xff) << 8) | (fl << 16), __float_as_int(rs));
-    }
     if (threadIdx.x == 0) {
         info[l] = make_int4(na, nt, np, lig.rec_idx[l]);
         rg[l] = lig.rg[l];
     }
 }
 
-// ------------------------------------------------------------------------------------------ per-warp workspace
-// Float offsets of the per-warp shared workspace for a given AM / KM (all float4 arrays first).
-struct WSLayout {
-    int X, FF, TT, ap, au, tp, tu, mk, ax, cs, sn, H, x, xn, xo, cur, best, g, gn, go, p, y, mhy, total;
-    __host__ __device__ WSLayout(int AM, int KM) {
-        const int DM = 6 + KM, SD = 7 + KM;
-        int o = 0;
-        X = o; o += 4 * AM;
-        FF = o; o += 4 * AM;
-        TT = o; o += 4 * AM;
-        ap = o; o += 4 * KM;
-        au = o; o += 4 * KM;
-        tp = o; o += 4 * KM;
-        tu = o; o += 4 * KM;
-        mk = o; o += AM;
-        ax = o; o += KM;      // packed axis atom indices (a0 | a1 << 16)
-        cs = o; o += KM;
-        sn = o; o += KM;
-        H = o; o += DM * DM;
-        x = o; o += SD;
-        xn = o; o += SD;
-        xo = o; o += SD;
-        cur = o; o += SD;
-        best = o; o += SD;
-        g = o; o += DM;
-        gn = o; o += DM;
-        go = o; o += DM;
-        p = o; o += DM;
-        y = o; o += DM;
-        mhy = o; o += DM;
-        total = (o + 3) & ~3;  // keep 16-byte alignment of the next warp
+// Intra-pair schedule (one warp per ligand): the np pairs are placed into R = ceil(np / 32) rounds of 32 slots so
+// that each atom appears as few times as possible per round. Greedy in pair order: among the rounds with a free
+// slot, the one where the larger of the two atoms' current counts is smallest (then their sum, then the lowest
+// round). Empty slots get x = -1. The force atomics of one round in eval_eg then collide at most a few ways
+// (small ligands cannot avoid it: a round of 32 pairs needs 64 atom slots).
+__global__ void schedule_pairs_kernel(adock_ligands_t lig, TypeTables tt, int2* pairs, int P_pad) {
+    __shared__ unsigned char cnt[PAIR_ROUNDS_MAX][128];
+    __shared__ int fill[PAIR_ROUNDS_MAX];
+    const int l = blockIdx.x, lane = threadIdx.x;
+    const int np = lig.np[l], AM = lig.AM, P = lig.P;
+    const int R = (np + 31) / 32;
+    int2* out = pairs + (long long)l * P_pad;
+    auto record = [&](int q) {
+        const int i = lig.pr[((long long)l * P + q) * 2], j = lig.pr[((long long)l * P + q) * 2 + 1];
+        int ti = lig.typ[(long long)l * AM + i], tj = lig.typ[(long long)l * AM + j];
+        ti = ti < 0 ? 0 : (ti & 63);
+        tj = tj < 0 ? 0 : (tj & 63);
+        const int fl = hyd_pair(tt.flags[ti], tt.flags[tj]) | hb_pair(tt.flags[ti], tt.flags[tj]);
+        return make_int2((i & 0xff) | ((j & 0xff) << 8) | (fl << 16), __float_as_int(tt.radius[ti] + tt.radius[tj]));
+    };
+    if (R > PAIR_ROUNDS_MAX) {  // very large ligands: keep the pair order
+        for (int q = lane; q < P_pad; q += 32) out[q] = q < np ? record(q) : make_int2(-1, 0);
+        return;
     }
-};
-
-// Per-chain context (registers).
-template <int APL>
-struct Chain {
-    int na, nt, np;
-    float rg;
-    const int2* pairs;
-    const char* grid;       // receptor's maps (bytes)
-    long long n3;
-    int ny, nz;
-    float o[3], lo[3], hi[3], fmx[3];
-    const float* rx;
-    const int* rt;
-    int rn;
-    const int* nb;
-    int nbn;
-    int exact;
-    // lane-owned atoms
-    float3 ref[APL];
-    int slot[APL];
-    int typ[APL];
-    uint32_t mask[APL];
-};
-
-template <int APL>
-__device__ __forceinline__ void load_chain(Chain<APL>& c, const SearchParams& P, int l, float* ws, const WSLayout& L,
-                                           int lane, int exact, const int* nb, int nbn) {
-    const int4 inf = P.info[l];
-    c.na = inf.x; c.nt = inf.y; c.np = inf.z;
-    const int ri = inf.w;
-    c.rg = P.rg[l];
-    c.pairs = P.pairs + (long long)l * P.P;
-    const long long nx = P.dims[3 * ri], ny = P.dims[3 * ri + 1], nz = P.dims[3 * ri + 2];
-    c.n3 = nx * ny * nz;
-    c.ny = (int)ny; c.nz = (int)nz;
-    c.grid = (const char*)P.flat;  // offset applied by the caller's element size
-    for (int d = 0; d < 3; ++d) {
-        c.o[d] = P.origin[3 * ri + d]; c.lo[d] = P.lo[3 * ri + d]; c.hi[d] = P.hi[3 * ri + d];
-    }
-    c.fmx[0] = (float)(nx - 1) - 1e-4f; c.fmx[1] = (float)(ny - 1) - 1e-4f; c.fmx[2] = (float)(nz - 1) - 1e-4f;
-    c.exact = exact;
-    c.rx = P.rxyz ? P.rxyz + (long long)ri * P.RN * 3 : nullptr;
-    c.rt = P.rtyp ? P.rtyp + (long long)ri * P.RN : nullptr;
-    c.rn = P.rn ? P.rn[ri] : 0;
-    c.nb = nb; c.nbn = nbn;
-    const float4* at = P.atoms + (long long)l * P.AM;
-    const uint32_t* mk = P.masks + (long long)l * P.AM;
-    uint32_t* smk = (uint32_t*)(ws + L.mk);
-#pragma unroll
-    for (int i = 0; i < APL; ++i) {
-        const int a = lane + 32 * i;
-        float4 v = at[a];
-        c.ref[i] = make_float3(v.x, v.y, v.z);
-        int meta = __float_as_int(v.w);
-        c.slot[i] = meta & 0xffff;
-        c.typ[i] = meta >> 16;
-        c.mask[i] = mk[a];
-        smk[a] = c.mask[i];
-    }
-    const float4* tr = P.tors + (long long)l * P.KM * 2;
-    float4* ap = (float4*)(ws + L.ap);
-    float4* au = (float4*)(ws + L.au);
-    int* axs = (int*)(ws + L.ax);
-    for (int k = lane; k < P.KM; k += 32) {
-        float4 p = tr[2 * k], u = tr[2 * k + 1];
-        ap[k] = p;
-        au[k] = u;
-        axs[k] = (__float_as_int(p.w) & 0xffff) | (__float_as_int(u.w) << 16);
+    for (int r = lane; r < PAIR_ROUNDS_MAX; r += 32) {
+        fill[r] = 0;
+        for (int a = 0; a < 128; ++a) cnt[r][a] = 0;
     }
     __syncwarp();
-}
-
-// trilinear lookup + analytic gradient of one atom (mckernel.py:140-149, :176-195)
-template <typename GT>
-__device__ __forceinline__ float trilinear(const GT* G, int ny, int nz, const float* o, const float* fmx, float inv_s,
-                                           float X0, float X1, float X2, float& gx, float& gy, float& gz) {
-    const float xx[3] = {X0, X1, X2};
-    float fw[3], inside[3];
-    int i0[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        float f = (xx[d] - o[d]) * inv_s;
-        float fc = fminf(fmaxf(f, 0.f), fmx[d]);
-        inside[d] = (f > 0.f && f < fmx[d]) ? 1.f : 0.f;
-        int ii = (int)floorf(fc);
-        i0[d] = ii;
-        fw[d] = fc - ii;
-    }
-    const long long b000 = ((long long)i0[0] * ny + i0[1]) * nz + i0[2];
-    const long long sx = (long long)ny * nz;
-    float v000 = gload(G + b000), v001 = gload(G + b000 + 1), v010 = gload(G + b000 + nz), v011 = gload(G + b000 + nz + 1);
-    float v100 = gload(G + b000 + sx), v101 = gload(G + b000 + sx + 1), v110 = gload(G + b000 + sx + nz),
-          v111 = gload(G + b000 + sx + nz + 1);
-    const float wx = fw[0], wy = fw[1], wz = fw[2];
-    float c00 = v000 * (1 - wz) + v001 * wz, c01 = v010 * (1 - wz) + v011 * wz;
-    float c10 = v100 * (1 - wz) + v101 * wz, c11 = v110 * (1 - wz) + v111 * wz;
-    float c0 = c00 * (1 - wy) + c01 * wy, c1 = c10 * (1 - wy) + c11 * wy;
-    float e = c0 * (1 - wx) + c1 * wx;
-    gx = (c1 - c0) * inv_s * inside[0];
-    gy = ((c01 - c00) * (1 - wx) + (c11 - c10) * wx) * inv_s * inside[1];
-    gz = (((v001 - v000) * (1 - wy) + (v011 - v010) * wy) * (1 - wx) + ((v101 - v100) * (1 - wy) + (v111 - v110) * wy) * wx) *
-         inv_s * inside[2];
-    return e;
-}
-
-// Energy + analytic pose gradient of state s (shared, SD floats) into g (shared, DM floats); E on all lanes.
-// Same energy as mckernel.py:108-244: torsions applied leaf -> root on reference coordinates, rotation,
-// translation; trilinear grid (or exact pairwise) inter energy with the quadratic out-of-box penalty; intra
-// pairs. Gradient: dE/dt = sum F, torque = sum (X - t) x F, dE/dtheta_k = u_k . sum_{a moved by k} (X_a - p_k) x F_a,
-// the last evaluated per torsion by one lane as u_k . (sum X' x F - p'_k x sum F) over its subtree (X' = X - t).
-template <int APL, typename GT>
-__device__ float eval_eg(float* ws, const WSLayout& L, const float* s, float* g, const Chain<APL>& c,
-                         const SearchParams& P, const TypeTables& tt, int lane) {
-    float4* X = (float4*)(ws + L.X);
-    float4* FF = (float4*)(ws + L.FF);
-    float4* TT = (float4*)(ws + L.TT);
-    const float4* ap = (const float4*)(ws + L.ap);
-    const float4* au = (const float4*)(ws + L.au);
-    float4* tp = (float4*)(ws + L.tp);
-    float4* tu = (float4*)(ws + L.tu);
-    const uint32_t* smk = (const uint32_t*)(ws + L.mk);
-    const int* axs = (const int*)(ws + L.ax);
-    float* cs = ws + L.cs;
-    float* sn = ws + L.sn;
-
-    const float t0 = s[0], t1 = s[1], t2 = s[2];
-    float qw = s[3], qx = s[4], qy = s[5], qz = s[6];
-    const float nq = rsqrtf(qw * qw + qx * qx + qy * qy + qz * qz);
-    qw *= nq; qx *= nq; qy *= nq; qz *= nq;
-    const float R00 = 1 - 2 * (qy * qy + qz * qz), R01 = 2 * (qx * qy - qz * qw), R02 = 2 * (qx * qz + qy * qw);
-    const float R10 = 2 * (qx * qy + qz * qw), R11 = 1 - 2 * (qx * qx + qz * qz), R12 = 2 * (qy * qz - qx * qw);
-    const float R20 = 2 * (qx * qz - qy * qw), R21 = 2 * (qy * qz + qx * qw), R22 = 1 - 2 * (qx * qx + qy * qy);
-    for (int k = lane; k < c.nt; k += 32) {
-        float sv, cv;
-        __sincosf(s[7 + k], &sv, &cv);
-        cs[k] = cv;
-        sn[k] = sv;
-    }
-    __syncwarp();
-    float e = 0.f;
-    const GT* grid = (const GT*)c.grid;
-#pragma unroll
-    for (int i = 0; i < APL; ++i) {
-        const int a = lane + 32 * i;
-        if (a < c.na) {
-            float px = c.ref[i].x, py = c.ref[i].y, pz = c.ref[i].z;
-            uint32_t m = c.mask[i];
-            while (m) {
-                const int k = __ffs(m) - 1;
-                m &= m - 1;
-                const float4 A = ap[k], U = au[k];
-                const float cv = cs[k], sv = sn[k];
-                float vx = px - A.x, vy = py - A.y, vz = pz - A.z;
-                float d = U.x * vx + U.y * vy + U.z * vz;
-                float cx = U.y * vz - U.z * vy, cy = U.z * vx - U.x * vz, cz = U.x * vy - U.y * vx;
-                px = A.x + vx * cv + cx * sv + U.x * d * (1 - cv);
-                py = A.y + vy * cv + cy * sv + U.y * d * (1 - cv);
-                pz = A.z + vz * cv + cz * sv + U.z * d * (1 - cv);
-            }
-            const float X0 = R00 * px + R01 * py + R02 * pz + t0;
-            const float X1 = R10 * px + R11 * py + R12 * pz + t1;
-            const float X2 = R20 * px + R21 * py + R22 * pz + t2;
-            X[a] = make_float4(X0, X1, X2, 0.f);
-            float ea, gg[3];
-            if (c.exact) {
-                ea = 0.f;
-                gg[0] = gg[1] = gg[2] = 0.f;
-                const int ta = c.typ[i];
-                const float ra = tt.radius[ta];
-                const int fa = tt.flags[ta];
-                const float cut2 = P.pp.cutoff * P.pp.cutoff;
-                const int nloop = c.nb ? c.nbn : c.rn;
-                for (int bb = 0; bb < nloop; ++bb) {
-                    const int b = c.nb ? c.nb[bb] : bb;
-                    float rx = X0 - c.rx[3 * b], ry = X1 - c.rx[3 * b + 1], rz = X2 - c.rx[3 * b + 2];
-                    float r2 = rx * rx + ry * ry + rz * rz;
-                    if (r2 >= cut2) continue;
-                    const int tb = c.rt[b] & 63;   // index kept inside the 64-entry type tables
-                    const int fb = tt.flags[tb];
-                    float r = sqrtf(r2), de;
-                    ea += pair_energy(r, ra + tt.radius[tb], hyd_pair(fa, fb) | hb_pair(fa, fb), P.pp, de);
-                    float sc = de / fmaxf(r, 1e-6f);
-                    gg[0] += sc * rx; gg[1] += sc * ry; gg[2] += sc * rz;
-                }
-            } else {
-                ea = trilinear<GT>(grid + (long long)c.slot[i] * c.n3, c.ny, c.nz, c.o, c.fmx, P.inv_s, X0, X1, X2, gg[0],
-                                   gg[1], gg[2]);
-            }
-            const float xx[3] = {X0, X1, X2};
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                float lo = fmaxf(c.lo[d] - xx[d], 0.f), hi = fmaxf(xx[d] - c.hi[d], 0.f);
-                ea += P.pen * (lo * lo + hi * hi);
-                gg[d] += P.pen * (-2.f * lo + 2.f * hi);
-            }
-            e += ea;
-            FF[a] = make_float4(gg[0], gg[1], gg[2], 0.f);
-        }
-    }
-    __syncwarp();
-    // intra-ligand pairs (forces accumulated into the owners' slots)
-    for (int q = lane; q < c.np; q += 32) {
-        const int2 pr = c.pairs[q];
-        const int i = pr.x & 0xff, j = (pr.x >> 8) & 0xff, fl = pr.x >> 16;
-        const float4 Xi = X[i], Xj = X[j];
-        float rx = Xi.x - Xj.x, ry = Xi.y - Xj.y, rz = Xi.z - Xj.z;
-        float r = sqrtf(rx * rx + ry * ry + rz * rz);
-        if (r >= P.pp.cutoff) continue;
-        float de;
-        e += pair_energy(r, __int_as_float(pr.y), fl, P.pp, de);
-        float sc = de / fmaxf(r, 1e-6f);
-        atomicAdd(&FF[i].x, sc * rx); atomicAdd(&FF[i].y, sc * ry); atomicAdd(&FF[i].z, sc * rz);
-        atomicAdd(&FF[j].x, -sc * rx); atomicAdd(&FF[j].y, -sc * ry); atomicAdd(&FF[j].z, -sc * rz);
-    }
-    // world torsion axes (axis atoms' current positions)
-    for (int k = lane; k < c.nt; k += 32) {
-        const int a0 = axs[k] & 0xffff, a1 = axs[k] >> 16;
-        const float4 A = X[a0], B = X[a1];
-        float ux = B.x - A.x, uy = B.y - A.y, uz = B.z - A.z;
-        float nn = rsqrtf(fmaxf(ux * ux + uy * uy + uz * uz, 1e-12f));
-        tp[k] = make_float4(A.x - t0, A.y - t1, A.z - t2, 0.f);
-        tu[k] = make_float4(ux * nn, uy * nn, uz * nn, 0.f);
-    }
-    __syncwarp();
-#pragma unroll
-    for (int i = 0; i < APL; ++i) {
-        const int a = lane + 32 * i;
-        if (a < c.na) {
-            const float4 F = FF[a], Xa = X[a];
-            const float dx = Xa.x - t0, dy = Xa.y - t1, dz = Xa.z - t2;
-            TT[a] = make_float4(dy * F.z - dz * F.y, dz * F.x - dx * F.z, dx * F.y - dy * F.x, 0.f);
-        }
-    }
-    __syncwarp();
-    // subtree sums: lane k < nt -> torsion k; lane k == nt -> whole ligand (force, torque)
-    for (int k = lane; k <= c.nt; k += 32) {
-        float S0 = 0.f, S1 = 0.f, S2 = 0.f, T0 = 0.f, T1 = 0.f, T2 = 0.f;
-        const bool all = (k == c.nt);
-        const uint32_t bit = all ? 0u : (1u << k);
-        for (int a = 0; a < c.na; ++a) {
-            if (all || (smk[a] & bit)) {
-                const float4 F = FF[a], T = TT[a];
-                S0 += F.x; S1 += F.y; S2 += F.z;
-                T0 += T.x; T1 += T.y; T2 += T.z;
+    for (int q = 0; q < np; ++q) {
+        const int i = lig.pr[((long long)l * P + q) * 2] & 127, j = lig.pr[((long long)l * P + q) * 2 + 1] & 127;
+        unsigned best = 0xffffffffu;
+        for (int r = lane; r < R; r += 32) {
+            if (fill[r] < 32) {
+                const unsigned ci = cnt[r][i], cj = cnt[r][j];
+                const unsigned key = (((ci > cj ? ci : cj) * 64u + ci + cj) << 16) | (unsigned)r;
+                best = key < best ? key : best;
             }
         }
-        if (all) {
-            g[0] = S0; g[1] = S1; g[2] = S2; g[3] = T0; g[4] = T1; g[5] = T2;
-        } else {
-            const float4 Pk = tp[k], Uk = tu[k];
-            const float cx = T0 - (Pk.y * S2 - Pk.z * S1);
-            const float cy = T1 - (Pk.z * S0 - Pk.x * S2);
-            const float cz = T2 - (Pk.x * S1 - Pk.y * S0);
-            g[6 + k] = cx * Uk.x + cy * Uk.y + cz * Uk.z;
-        }
-    }
-    e = warp_sum(e);
-    __syncwarp();
-    return e;
-}
-
-__device__ __forceinline__ float wdot(const float* a, const float* b, int D, int lane) {
-    float s = 0.f;
-    for (int i = lane; i < D; i += 32) s += a[i] * b[i];
-    return warp_sum(s);
-}
-__device__ __forceinline__ double wdot64(const float* a, const float* b, int D, int lane) {
-    double s = 0.0;
-    for (int i = lane; i < D; i += 32) s += (double)a[i] * (double)b[i];
-    return warp_sum_d(s);
-}
-__device__ __forceinline__ void wcopy(float* dst, const float* src, int D, int lane) {
-    for (int i = lane; i < D; i += 32) dst[i] = src[i];
-    __syncwarp();
-}
-// xn = x (+) alpha p: translation add, rotation-vector increment of the quaternion, torsion add (mckernel.py:256-265)
-__device__ __forceinline__ void conf_step(float* xn, const float* x, const float* p, float alpha, int nt, int lane) {
-    if (lane == 0) {
-        xn[0] = x[0] + alpha * p[0]; xn[1] = x[1] + alpha * p[1]; xn[2] = x[2] + alpha * p[2];
-        xn[3] = x[3]; xn[4] = x[4]; xn[5] = x[5]; xn[6] = x[6];
-        quat_apply_rotvec(xn + 3, alpha * p[3], alpha * p[4], alpha * p[5]);
-    }
-    for (int k = lane; k < nt; k += 32) xn[7 + k] = x[7 + k] + alpha * p[6 + k];
-    __syncwarp();
-}
-
-// Vina-1.2-style BFGS on state x (shared, in/out); returns the final energy (mckernel.py:267-326).
-// The curvature scalar y.p and the update guard alpha * y.p >= eps are evaluated in float64.
-template <int APL, typename GT>
-__device__ float bfgs(float* ws, const WSLayout& L, float* x, int iters, const Chain<APL>& c, const SearchParams& P,
-                      const TypeTables& tt, int lane, unsigned& n_eval) {
-    const int D = 6 + c.nt, S = 7 + c.nt;
-    float* H = ws + L.H;
-    float* g = ws + L.g;
-    float* gn = ws + L.gn;
-    float* go = ws + L.go;
-    float* p = ws + L.p;
-    float* y = ws + L.y;
-    float* mhy = ws + L.mhy;
-    float* xn = ws + L.xn;
-    float* xo = ws + L.xo;
-    float f0 = eval_eg<APL, GT>(ws, L, x, g, c, P, tt, lane);
-    ++n_eval;
-    const float f_orig = f0;
-    wcopy(xo, x, S, lane);
-    wcopy(go, g, D, lane);
-    // H is symmetric: stored with column index fastest, lane i owns column i
-    for (int i = lane; i < D; i += 32)
-        for (int j = 0; j < D; ++j) H[j * D + i] = (i == j) ? 1.f : 0.f;
-    __syncwarp();
-    for (int step = 0; step < iters; ++step) {
-        for (int i = lane; i < D; i += 32) {
-            float acc = 0.f;
-            for (int j = 0; j < D; ++j) acc += H[j * D + i] * g[j];
-            p[i] = -acc;
-        }
-        __syncwarp();
-        const float pg = wdot(p, g, D, lane);
-        float alpha = 1.f, f1 = 0.f;
-        for (int trial = 0; trial < 10; ++trial) {
-            conf_step(xn, x, p, alpha, c.nt, lane);
-            f1 = eval_eg<APL, GT>(ws, L, xn, gn, c, P, tt, lane);
-            ++n_eval;
-            if (f1 - f0 < 1e-4f * alpha * pg) break;
-            alpha *= 0.5f;
-        }
-        for (int i = lane; i < D; i += 32) y[i] = gn[i] - g[i];
-        __syncwarp();
-        f0 = f1;
-        wcopy(x, xn, S, lane);
-        const float gg = wdot(gn, gn, D, lane);
-        wcopy(g, gn, D, lane);
-        if (!(sqrtf(gg) >= 1e-5f)) break;
-        const double yp = wdot64(y, p, D, lane);
-        if (step == 0) {
-            const float yy = wdot(y, y, D, lane);
-            if (fabsf(yy) > EPSF) {
-                const float dg = (float)((double)alpha * yp / (double)yy);
-                for (int i = lane; i < D; i += 32)
-                    for (int j = 0; j < D; ++j) H[j * D + i] = (i == j) ? dg : 0.f;
-                __syncwarp();
-            }
-        }
-        const double ayp = (double)alpha * yp;
-        if (ayp < (double)EPSF) continue;
-        for (int i = lane; i < D; i += 32) {
-            float acc = 0.f;
-            for (int j = 0; j < D; ++j) acc += H[j * D + i] * y[j];
-            mhy[i] = -acc;
-        }
-        __syncwarp();
-        const float yhy = -wdot(y, mhy, D, lane);
-        const float r = (float)(1.0 / ayp);
-        const float c2 = alpha * alpha * (r * r * yhy + r);
-        const float ar = alpha * r;
-        for (int i = lane; i < D; i += 32) {
-            const float mi = mhy[i], pi = p[i];
-            for (int j = 0; j < D; ++j) H[j * D + i] += ar * (mi * p[j] + mhy[j] * pi) + c2 * pi * p[j];
-        }
-        __syncwarp();
-    }
-    if (!(f0 <= f_orig)) {
-        f0 = f_orig;
-        wcopy(x, xo, S, lane);
-        wcopy(g, go, D, lane);
-    }
-    return f0;
-}
-
-struct McParams {
-    const int* chain_lig;
-    const int* chain_id;
-    int n_chains;
-    const int* nbr;
-    const int* nbr_n;
-    int nb_max;
-    float* cur;
-    float* cur_e;
-    float* best;
-    float* best_e;
-    int init_opt, mc_steps, bfgs_iters;
-    float temp, amp_pos, amp_rot;
-    unsigned long long seed;
-    int step_offset;
-    int exact;
-    const int* order;
-    int* queue;
-    unsigned long long* evals;
-};
-
-__device__ __forceinline__ void stage_tables(TypeTables& dst, const TypeTables& src) {
-    for (int i = threadIdx.x; i < 64; i += blockDim.x) {
-        dst.radius[i] = src.radius[i];
-        dst.flags[i] = src.flags[i];
-    }
-    __syncthreads();
-}
-
-template <int APL, typename GT>
-__global__ void __launch_bounds__(128) mc_kernel(const __grid_constant__ SearchParams P, const __grid_constant__ McParams M,
-                                                 const __grid_constant__ TypeTables ttg) {
-    extern __shared__ float4 smem4[];
-    __shared__ TypeTables tt;
-    stage_tables(tt, ttg);
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const WSLayout L(P.AM, P.KM);
-    float* ws = (float*)smem4 + (size_t)wid * L.total;
-    const int SDM = 7 + P.KM;
-    unsigned n_eval = 0;
-    unsigned long long n_atom_eval = 0;
-    while (true) {
-        int idx = 0;
-        if (lane == 0) idx = atomicAdd(M.queue, 1);
-        idx = __shfl_sync(0xffffffffu, idx, 0);
-        if (idx >= M.n_chains) break;
-        const int ch = M.order ? M.order[idx] : idx;
-        const int l = M.chain_lig[ch];
-        const int cid = M.chain_id[ch];
-        const unsigned n_eval_start = n_eval;
-        Chain<APL> c;
-        const int* nb = M.nbr ? M.nbr + (long long)ch * M.nb_max : nullptr;
-        const int nbn = M.nbr ? M.nbr_n[ch] : 0;
-        load_chain<APL>(c, P, l, ws, L, lane, M.exact, nb, nbn);
-        const int ri = P.info[l].w;
-        c.grid = (const char*)((const GT*)P.flat + P.offs[ri]);
-        const int S = 7 + c.nt;
-        const int iters = M.bfgs_iters > 0 ? M.bfgs_iters : (25 + c.na) / 3;
-        float* cur = ws + L.cur;
-        float* best = ws + L.best;
-        float* x = ws + L.x;
-        float* gcur = M.cur + (long long)ch * SDM;
-        float* gbest = M.best + (long long)ch * SDM;
-        for (int i = lane; i < S; i += 32) {
-            cur[i] = gcur[i];
-            best[i] = gbest[i];
-        }
-        __syncwarp();
-        float ec, eb = M.best_e[ch];
-        if (M.init_opt) ec = bfgs<APL, GT>(ws, L, cur, iters, c, P, tt, lane, n_eval);
-        else ec = M.cur_e[ch];
-        if (ec < eb) {
-            eb = ec;
-            wcopy(best, cur, S, lane);
-        }
-        for (int st = 0; st < M.mc_steps; ++st) {
-            const int sg = M.step_offset + st;
-            wcopy(x, cur, S, lane);
-            const int nm = 2 + c.nt;
-            const int which = min((int)(uniform01(M.seed, cid, sg, 0) * nm), nm - 1);
-            if (lane == 0) {
-                float v[3];
-                if (which == 0) {
-                    unit_ball(M.seed, cid, sg, 10, v);
-                    x[0] += M.amp_pos * v[0]; x[1] += M.amp_pos * v[1]; x[2] += M.amp_pos * v[2];
-                } else if (which == 1) {
-                    unit_ball(M.seed, cid, sg, 10, v);
-                    const float sc = M.amp_rot / fmaxf(c.rg, 1.0f);
-                    quat_apply_rotvec(x + 3, sc * v[0], sc * v[1], sc * v[2]);
-                } else {
-                    x[7 + which - 2] = (2.f * uniform01(M.seed, cid, sg, 1) - 1.f) * 3.14159265f;
-                }
-            }
-            __syncwarp();
-            const float en = bfgs<APL, GT>(ws, L, x, iters, c, P, tt, lane, n_eval);
-            const bool accept = (en < ec) || (uniform01(M.seed, cid, sg, 2) < __expf((ec - en) / M.temp));
-            if (accept) {
-                ec = en;
-                wcopy(cur, x, S, lane);
-                if (en < eb) {
-                    eb = en;
-                    wcopy(best, x, S, lane);
-                }
-            }
-        }
-        for (int i = lane; i < S; i += 32) {
-            gcur[i] = cur[i];
-            gbest[i] = best[i];
-        }
+        best = __reduce_min_sync(0xffffffffu, best);
+        const int found = (int)(best & 0xffffu);
         if (lane == 0) {
-            M.cur_e[ch] = ec;
-            M.best_e[ch] = eb;
+            const int slot = found * 32 + fill[found];
+            fill[found] += 1;
+            cnt[found][i] += 1;
+            cnt[found][j] += 1;
+            out[slot] = record(q);
         }
-        n_atom_eval += (unsigned long long)(n_eval - n_eval_start) * c.na;
         __syncwarp();
     }
-    if (M.evals && lane == 0 && n_eval) {
-        atomicAdd(&M.evals[0], (unsigned long long)n_eval);
-        atomicAdd(&M.evals[1], n_atom_eval);
-    }
-}
-
-template <int APL, typename GT>
-__global__ void __launch_bounds__(128) eg_kernel(const __grid_constant__ SearchParams P, const int* chain_lig, int n,
-                                                 const float* state, float* e_out, float* g_out, int exact,
-                                                 const __grid_constant__ TypeTables ttg) {
-    extern __shared__ float4 smem4[];
-    __shared__ TypeTables tt;
-    stage_tables(tt, ttg);
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const WSLayout L(P.AM, P.KM);
-    float* ws = (float*)smem4 + (size_t)wid * L.total;
-    const int SDM = 7 + P.KM, DMM = 6 + P.KM;
-    const int warps = (blockDim.x >> 5) * gridDim.x;
-    for (int ch = blockIdx.x * (blockDim.x >> 5) + wid; ch < n; ch += warps) {
-        const int l = chain_lig[ch];
-        Chain<APL> c;
-        load_chain<APL>(c, P, l, ws, L, lane, exact, nullptr, 0);
-        const int ri = P.info[l].w;
-        c.grid = (const char*)((const GT*)P.flat + P.offs[ri]);
-        float* x = ws + L.x;
-        float* g = ws + L.g;
-        for (int i = lane; i < SDM; i += 32) x[i] = state[(long long)ch * SDM + i];
-        __syncwarp();
-        const float e = eval_eg<APL, GT>(ws, L, x, g, c, P, tt, lane);
-        for (int i = lane; i < 6 + c.nt; i += 32) g_out[(long long)ch * DMM + i] = g[i];
-        if (lane == 0) e_out[ch] = e;
-        __syncwarp();
-    }
-}
-
-// ------------------------------------------------------------------------------------------ Stage A
-// Block = (ligand l, conformer c, rotation q); threads over lattice translations; e(T) = sum_a min(cap,
-// nearest-grid energy + out-of-box penalty); block min and argmin (ties -> lowest index), mckernel.py:451-521.
-template <typename GT>
-__global__ void __launch_bounds__(256) stage_a_kernel(const __grid_constant__ SearchParams P, const float* conf, int C,
-                                                      const float* quats, int Q, const float* trans,
-                                                      const int* ntrans, int NT_MAX, float cap, float* best_e,
-                                                      int* best_i) {
-    extern __shared__ float4 smem4[];
-    float4* X = smem4;                               // [AM] rotated conformer + slot bits
-    __shared__ float red_e[256];
-    __shared__ int red_i[256];
-    const long long b = blockIdx.x;
-    const int q = (int)(b % Q);
-    const int cc = (int)((b / Q) % C);
-    const int l = (int)(b / ((long long)Q * C));
-    const int4 inf = P.info[l];
-    const int n_at = inf.x, ri = inf.w;
-    float qw = quats[4 * q], qx = quats[4 * q + 1], qy = quats[4 * q + 2], qz = quats[4 * q + 3];
-    const float nq = rsqrtf(qw * qw + qx * qx + qy * qy + qz * qz);
-    qw *= nq; qx *= nq; qy *= nq; qz *= nq;
-    for (int a = threadIdx.x; a < n_at; a += blockDim.x) {
-        const float* p = conf + (((long long)l * C + cc) * P.AM + a) * 3;
-        const float px = p[0], py = p[1], pz = p[2];
-        const int slot = __float_as_int(P.atoms[(long long)l * P.AM + a].w) & 0xffff;
-        X[a] = make_float4((1 - 2 * (qy * qy + qz * qz)) * px + 2 * (qx * qy - qz * qw) * py + 2 * (qx * qz + qy * qw) * pz,
-                           2 * (qx * qy + qz * qw) * px + (1 - 2 * (qx * qx + qz * qz)) * py + 2 * (qy * qz - qx * qw) * pz,
-                           2 * (qx * qz - qy * qw) * px + 2 * (qy * qz + qx * qw) * py + (1 - 2 * (qx * qx + qy * qy)) * pz,
-                           __int_as_float(slot));
-    }
-    __syncthreads();
-    const GT* G = (const GT*)P.flat + P.offs[ri];
-    const int nx = (int)P.dims[3 * ri], ny = (int)P.dims[3 * ri + 1], nz = (int)P.dims[3 * ri + 2];
-    const long long n3 = (long long)nx * ny * nz;
-    const float ox = P.origin[3 * ri], oy = P.origin[3 * ri + 1], oz = P.origin[3 * ri + 2];
-    const float lx = P.lo[3 * ri], ly = P.lo[3 * ri + 1], lz = P.lo[3 * ri + 2];
-    const float hx = P.hi[3 * ri], hy = P.hi[3 * ri + 1], hz = P.hi[3 * ri + 2];
-    const float inv = P.inv_s, pen = P.pen;
-    float be = 3.4e38f;
-    int bi = 0;
-    const int nT = ntrans[l];
-    for (int ti = threadIdx.x; ti < nT; ti += blockDim.x) {
-        const float* T = trans + ((long long)l * NT_MAX + ti) * 3;
-        const float T0 = T[0], T1 = T[1], T2 = T[2];
-        float e = 0.f;
-        for (int a = 0; a < n_at; ++a) {
-            const float4 v = X[a];
-            const float x = v.x + T0, y = v.y + T1, z = v.z + T2;
-            const int i = min(max(__float2int_rn((x - ox) * inv), 0), nx - 1);
-            const int j = min(max(__float2int_rn((y - oy) * inv), 0), ny - 1);
-            const int k = min(max(__float2int_rn((z - oz) * inv), 0), nz - 1);
-            float ea = gload(G + (long long)__float_as_int(v.w) * n3 + ((long long)i * ny + j) * nz + k);
-            const float dx0 = fmaxf(lx - x, 0.f), dx1 = fmaxf(x - hx, 0.f);
-            const float dy0 = fmaxf(ly - y, 0.f), dy1 = fmaxf(y - hy, 0.f);
-            const float dz0 = fmaxf(lz - z, 0.f), dz1 = fmaxf(z - hz, 0.f);
-            ea += pen * (dx0 * dx0 + dx1 * dx1 + dy0 * dy0 + dy1 * dy1 + dz0 * dz0 + dz1 * dz1);
-            e += fminf(ea, cap);
-        }
-        if (e < be) { be = e; bi = ti; }
-    }
-    red_e[threadIdx.x] = be;
-    red_i[threadIdx.x] = bi;
-    __syncthreads();
-    for (int sft = blockDim.x / 2; sft > 0; sft >>= 1) {
-        if (threadIdx.x < sft) {
-            const float o = red_e[threadIdx.x + sft];
-            const int oi = red_i[threadIdx.x + sft];
-            if (o < red_e[threadIdx.x] || (o == red_e[threadIdx.x] && oi < red_i[threadIdx.x])) {
-                red_e[threadIdx.x] = o;
-                red_i[threadIdx.x] = oi;
-            }
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        best_e[b] = red_e[0];
-        best_i[b] = red_i[0];
+    for (int q = lane; q < P_pad; q += 32) {
+        const int r = q >> 5;
+        if (r >= R || (q & 31) >= fill[r]) out[q] = make_int2(-1, 0);
     }
 }
 
 // ------------------------------------------------------------------------------------------ pose coordinates
 // World coordinates of the heavy atoms of one state (one warp), float32 path of eval_eg.
-__device__ void pose_world(const SearchParams& P, int l, const float* s, float4* Xout, float4* axs_sh, int lane) {
+__device__ void pose_world(const SearchParams& P, int l, const float* s, float4* Xout, int lane) {
     const int4 inf = P.info[l];
     const int na = inf.x, nt = inf.y;
     float qw = s[3], qx = s[4], qy = s[5], qz = s[6];
@@ -747,9 +122,9 @@ __device__ void pose_world(const SearchParams& P, int l, const float* s, float4*
             const float4 A = tr[2 * k], U = tr[2 * k + 1];
             float sv, cv;
             __sincosf(s[7 + k], &sv, &cv);
-            float vx = px - A.x, vy = py - A.y, vz = pz - A.z;
-            float d = U.x * vx + U.y * vy + U.z * vz;
-            float cx = U.y * vz - U.z * vy, cy = U.z * vx - U.x * vz, cz = U.x * vy - U.y * vx;
+            const float vx = px - A.x, vy = py - A.y, vz = pz - A.z;
+            const float d = U.x * vx + U.y * vy + U.z * vz;
+            const float cx = U.y * vz - U.z * vy, cy = U.z * vx - U.x * vz, cz = U.x * vy - U.y * vx;
             px = A.x + vx * cv + cx * sv + U.x * d * (1 - cv);
             py = A.y + vy * cv + cy * sv + U.y * d * (1 - cv);
             pz = A.z + vz * cv + cz * sv + U.z * d * (1 - cv);
@@ -763,8 +138,8 @@ __device__ void pose_world(const SearchParams& P, int l, const float* s, float4*
 // ------------------------------------------------------------------------------------------ neighbour lists
 // Block per chain: heavy-atom world coordinates in shared memory, threads over receptor atoms; pass 1 counts,
 // pass 2 writes the indices in receptor order (ordered block compaction).
-__global__ void __launch_bounds__(256) neighbours_kernel(const __grid_constant__ SearchParams P, const int* chain_lig, int n,
-                                                         const float* state, float cut2, int* nbr, int* nbr_n,
+__global__ void __launch_bounds__(256) neighbours_kernel(const __grid_constant__ SearchParams P, const int* chain_lig,
+                                                         int n, const float* state, float cut2, int* nbr, int* nbr_n,
                                                          int nb_max) {
     extern __shared__ float4 smem4[];
     float4* X = smem4;  // [AM]
@@ -778,7 +153,7 @@ __global__ void __launch_bounds__(256) neighbours_kernel(const __grid_constant__
     const int na = inf.x, ri = inf.w;
     for (int i = threadIdx.x; i < 7 + min(P.KM, 32); i += blockDim.x) s[i] = state[(long long)ch * SDM + i];
     __syncthreads();
-    if (threadIdx.x < 32) pose_world(P, l, s, X, nullptr, threadIdx.x);
+    if (threadIdx.x < 32) pose_world(P, l, s, X, threadIdx.x);
     __syncthreads();
     const float* rx = P.rxyz + (long long)ri * P.RN * 3;
     const int rn = P.rn[ri];
@@ -816,124 +191,6 @@ __global__ void __launch_bounds__(256) neighbours_kernel(const __grid_constant__
     if (threadIdx.x == 0) nbr_n[ch] = base_sh;
 }
 
-// ------------------------------------------------------------------------------------------ float64 re-score
-// One warp per state: float64 forward kinematics, exact pairwise inter energy over all receptor atoms (or the
-// float grid interpolated in float64 when no receptor atoms are given), out-of-box penalty, intra pairs.
-template <typename GT>
-__global__ void __launch_bounds__(128) rescore64_kernel(const __grid_constant__ SearchParams P, const int* chain_lig, int n,
-                                                        const float* state, double* e_total, double* e_intra,
-                                                        float* Xout, const __grid_constant__ TypeTables ttg,
-                                                        const __grid_constant__ adock_sf_t sf) {
-    extern __shared__ double smemd[];
-    __shared__ TypeTables tt;
-    stage_tables(tt, ttg);
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    double* X = smemd + (size_t)wid * P.AM * 3;
-    const int SDM = 7 + P.KM;
-    const int ch = blockIdx.x * (blockDim.x >> 5) + wid;
-    if (ch >= n) return;
-    const int l = chain_lig[ch];
-    const int4 inf = P.info[l];
-    const int na = inf.x, nt = inf.y, np = inf.z, ri = inf.w;
-    const float* s = state + (long long)ch * SDM;
-    double qw = s[3], qx = s[4], qy = s[5], qz = s[6];
-    const double nq = 1.0 / sqrt(qw * qw + qx * qx + qy * qy + qz * qz);
-    qw *= nq; qx *= nq; qy *= nq; qz *= nq;
-    const double R00 = 1 - 2 * (qy * qy + qz * qz), R01 = 2 * (qx * qy - qz * qw), R02 = 2 * (qx * qz + qy * qw);
-    const double R10 = 2 * (qx * qy + qz * qw), R11 = 1 - 2 * (qx * qx + qz * qz), R12 = 2 * (qy * qz - qx * qw);
-    const double R20 = 2 * (qx * qz - qy * qw), R21 = 2 * (qy * qz + qx * qw), R22 = 1 - 2 * (qx * qx + qy * qy);
-    const float4* tr = P.tors + (long long)l * P.KM * 2;
-    double einter = 0.0, eintra = 0.0;
-    const double cut = P.pp.cutoff;
-    for (int a = lane; a < na; a += 32) {
-        const float4 v = P.atoms[(long long)l * P.AM + a];
-        double px = v.x, py = v.y, pz = v.z;
-        uint32_t m = P.masks[(long long)l * P.AM + a];
-        while (m) {
-            const int k = __ffs(m) - 1;
-            m &= m - 1;
-            if (k >= nt) break;
-            const float4 A = tr[2 * k], U = tr[2 * k + 1];
-            double sv, cv;
-            sincos((double)s[7 + k], &sv, &cv);
-            double vx = px - A.x, vy = py - A.y, vz = pz - A.z;
-            double d = U.x * vx + U.y * vy + U.z * vz;
-            double cx = U.y * vz - U.z * vy, cy = U.z * vx - U.x * vz, cz = U.x * vy - U.y * vx;
-            px = A.x + vx * cv + cx * sv + U.x * d * (1 - cv);
-            py = A.y + vy * cv + cy * sv + U.y * d * (1 - cv);
-            pz = A.z + vz * cv + cz * sv + U.z * d * (1 - cv);
-        }
-        const double X0 = R00 * px + R01 * py + R02 * pz + s[0];
-        const double X1 = R10 * px + R11 * py + R12 * pz + s[1];
-        const double X2 = R20 * px + R21 * py + R22 * pz + s[2];
-        X[3 * a] = X0; X[3 * a + 1] = X1; X[3 * a + 2] = X2;
-        Xout[((long long)ch * P.AM + a) * 3] = (float)X0;
-        Xout[((long long)ch * P.AM + a) * 3 + 1] = (float)X1;
-        Xout[((long long)ch * P.AM + a) * 3 + 2] = (float)X2;
-        const int meta = __float_as_int(v.w);
-        const int ta = meta >> 16, slot = meta & 0xffff;
-        double ea = 0.0;
-        if (P.rxyz) {
-            const float* rx = P.rxyz + (long long)ri * P.RN * 3;
-            const int* rt = P.rtyp + (long long)ri * P.RN;
-            const int rn = P.rn[ri];
-            const int fa = tt.flags[ta];
-            for (int b = 0; b < rn; ++b) {
-                const double dx = X0 - rx[3 * b], dy = X1 - rx[3 * b + 1], dz = X2 - rx[3 * b + 2];
-                const double r2 = dx * dx + dy * dy + dz * dz;
-                if (r2 >= cut * cut) continue;
-                const int tb = rt[b] & 63, fb = tt.flags[tb];
-                ea += pair_energy64(sqrt(r2), (double)tt.radius[ta] + (double)tt.radius[tb],
-                                    hyd_pair(fa, fb) | hb_pair(fa, fb), sf.prm);
-            }
-        } else {
-            const GT* G = (const GT*)P.flat + P.offs[ri];
-            const long long nx = P.dims[3 * ri], ny = P.dims[3 * ri + 1], nz = P.dims[3 * ri + 2];
-            const double xx[3] = {X0, X1, X2};
-            const double nn[3] = {(double)nx, (double)ny, (double)nz};
-            double fw[3];
-            long long i0[3];
-            for (int d = 0; d < 3; ++d) {
-                double f = (xx[d] - P.origin[3 * ri + d]) / (double)(1.0f / P.inv_s);
-                double fc = fmin(fmax(f, 0.0), nn[d] - 1.0 - 1e-4);
-                i0[d] = (long long)floor(fc);
-                fw[d] = fc - (double)i0[d];
-            }
-            const GT* Gs = G + (long long)slot * nx * ny * nz;
-            for (int dx = 0; dx < 2; ++dx)
-                for (int dy = 0; dy < 2; ++dy)
-                    for (int dz = 0; dz < 2; ++dz) {
-                        const double w = (dx ? fw[0] : 1 - fw[0]) * (dy ? fw[1] : 1 - fw[1]) * (dz ? fw[2] : 1 - fw[2]);
-                        ea += w * (double)gload(Gs + ((i0[0] + dx) * ny + (i0[1] + dy)) * nz + (i0[2] + dz));
-                    }
-        }
-        const double xx[3] = {X0, X1, X2};
-        for (int d = 0; d < 3; ++d) {
-            const double lo = fmax((double)P.lo[3 * ri + d] - xx[d], 0.0), hi = fmax(xx[d] - (double)P.hi[3 * ri + d], 0.0);
-            ea += (double)P.pen * (lo * lo + hi * hi);
-        }
-        einter += ea;
-    }
-    __syncwarp();
-    const int2* pairs = P.pairs + (long long)l * P.P;
-    for (int q = lane; q < np; q += 32) {
-        const int2 pr = pairs[q];
-        const int i = pr.x & 0xff, j = (pr.x >> 8) & 0xff, fl = pr.x >> 16;
-        const double dx = X[3 * i] - X[3 * j], dy = X[3 * i + 1] - X[3 * j + 1], dz = X[3 * i + 2] - X[3 * j + 2];
-        const double r = sqrt(dx * dx + dy * dy + dz * dz);
-        if (r >= cut) continue;
-        const int ti = __float_as_int(P.atoms[(long long)l * P.AM + i].w) >> 16;
-        const int tj = __float_as_int(P.atoms[(long long)l * P.AM + j].w) >> 16;
-        eintra += pair_energy64(r, (double)tt.radius[ti] + (double)tt.radius[tj], fl, sf.prm);
-    }
-    einter = warp_sum_d(einter);
-    eintra = warp_sum_d(eintra);
-    if (lane == 0) {
-        e_total[ch] = einter + eintra;
-        e_intra[ch] = eintra;
-    }
-}
-
 // ------------------------------------------------------------------------------------------ host side
 static TypeTables make_tables(const adock_sf_t* sf) {
     TypeTables t;
@@ -949,6 +206,7 @@ static int make_params(SearchParams& P, const adock_ligands_t* lig, const adock_
     ADOCK_CHECK_ARG(lig && work && sf, "null ligand/work/sf argument");
     ADOCK_CHECK_ARG(lig->AM % 32 == 0 && lig->AM >= 32 && lig->AM <= 128, "AM must be 32, 64, 96 or 128 (got %d)", lig->AM);
     ADOCK_CHECK_ARG(lig->KM >= 1 && lig->KM <= 32, "KM must be in [1, 32] (got %d)", lig->KM);
+    ADOCK_CHECK_ARG(lig->P >= 1, "P must be >= 1");
     ADOCK_CHECK_ARG(sf->n_types >= 1 && sf->n_types <= 64, "n_types must be in [1, 64]");
     P.atoms = (const float4*)work->atoms;
     P.masks = (const uint32_t*)work->masks;
@@ -956,7 +214,7 @@ static int make_params(SearchParams& P, const adock_ligands_t* lig, const adock_
     P.pairs = (const int2*)work->pairs;
     P.info = (const int4*)work->info;
     P.rg = (const float*)work->rg;
-    P.AM = lig->AM; P.KM = lig->KM; P.P = lig->P;
+    P.AM = lig->AM; P.KM = lig->KM; P.P = lig->P; P.P_pad = pad32(lig->P);
     if (grids) {
         P.flat = grids->flat; P.offs = grids->offs; P.dims = grids->dims;
         P.origin = grids->origin; P.lo = grids->lo; P.hi = grids->hi;
@@ -975,62 +233,6 @@ static int make_params(SearchParams& P, const adock_ligands_t* lig, const adock_
     return ADOCK_OK;
 }
 
-template <int APL, typename GT>
-static int launch_mc_t(const SearchParams& P, const McParams& M, const TypeTables& tt, cudaStream_t st, int wpb) {
-    const WSLayout L(P.AM, P.KM);
-    const size_t smem = (size_t)wpb * L.total * sizeof(float);
-    auto kern = mc_kernel<APL, GT>;
-    ADOCK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0;
-    ADOCK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * wpb, smem));
-    if (per_sm < 1) per_sm = 1;
-    long long blocks = (long long)sm_count() * per_sm;
-    const long long need = (M.n_chains + wpb - 1) / wpb;
-    if (blocks > need) blocks = need;
-    if (blocks < 1) blocks = 1;
-    ADOCK_CUDA(cudaMemsetAsync(M.queue, 0, sizeof(int), st));
-    kern<<<(unsigned)blocks, 32 * wpb, smem, st>>>(P, M, tt);
-    ADOCK_CUDA(cudaGetLastError());
-    return ADOCK_OK;
-}
-
-template <typename GT>
-static int launch_mc_apl(const SearchParams& P, const McParams& M, const TypeTables& tt, cudaStream_t st, int wpb) {
-    switch (P.AM / 32) {
-        case 1: return launch_mc_t<1, GT>(P, M, tt, st, wpb);
-        case 2: return launch_mc_t<2, GT>(P, M, tt, st, wpb);
-        case 3: return launch_mc_t<3, GT>(P, M, tt, st, wpb);
-        default: return launch_mc_t<4, GT>(P, M, tt, st, wpb);
-    }
-}
-
-template <int APL, typename GT>
-static int launch_eg_t(const SearchParams& P, const int* cl, int n, const float* state, float* e, float* g, int exact,
-                       const TypeTables& tt, cudaStream_t st) {
-    const int wpb = 4;
-    const WSLayout L(P.AM, P.KM);
-    const size_t smem = (size_t)wpb * L.total * sizeof(float);
-    auto kern = eg_kernel<APL, GT>;
-    ADOCK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    long long blocks = (n + wpb - 1) / wpb;
-    const long long cap = (long long)sm_count() * 16;
-    if (blocks > cap) blocks = cap;
-    kern<<<(unsigned)blocks, 32 * wpb, smem, st>>>(P, cl, n, state, e, g, exact, tt);
-    ADOCK_CUDA(cudaGetLastError());
-    return ADOCK_OK;
-}
-
-template <typename GT>
-static int launch_eg_apl(const SearchParams& P, const int* cl, int n, const float* state, float* e, float* g, int exact,
-                         const TypeTables& tt, cudaStream_t st) {
-    switch (P.AM / 32) {
-        case 1: return launch_eg_t<1, GT>(P, cl, n, state, e, g, exact, tt, st);
-        case 2: return launch_eg_t<2, GT>(P, cl, n, state, e, g, exact, tt, st);
-        case 3: return launch_eg_t<3, GT>(P, cl, n, state, e, g, exact, tt, st);
-        default: return launch_eg_t<4, GT>(P, cl, n, state, e, g, exact, tt, st);
-    }
-}
-
 }  // namespace adock
 
 using namespace adock;
@@ -1043,10 +245,12 @@ extern "C" int adock_prepare(const adock_ligands_t* lig, const adock_sf_t* sf, a
     ADOCK_CHECK_ARG(lig->P >= 1, "P must be >= 1");
     ADOCK_CHECK_ARG(sf->n_types >= 1 && sf->n_types <= 64, "n_types must be in [1, 64]");
     ADOCK_CHECK_ARG(work->atoms && work->masks && work->tors && work->pairs && work->info && work->rg, "null work buffer");
-    TypeTables tt = make_tables(sf);
-    prepare_kernel<<<lig->L, 128, 0, (cudaStream_t)stream>>>(*lig, tt, (float4*)work->atoms, (uint32_t*)work->masks,
-                                                             (float4*)work->tors, (int2*)work->pairs, (int4*)work->info,
-                                                             (float*)work->rg);
+    const TypeTables tt = make_tables(sf);
+    cudaStream_t st = (cudaStream_t)stream;
+    prepare_kernel<<<lig->L, 128, 0, st>>>(*lig, tt, (float4*)work->atoms, (uint32_t*)work->masks, (float4*)work->tors,
+                                           (int4*)work->info, (float*)work->rg);
+    ADOCK_CUDA(cudaGetLastError());
+    schedule_pairs_kernel<<<lig->L, 32, 0, st>>>(*lig, tt, (int2*)work->pairs, pad32(lig->P));
     ADOCK_CUDA(cudaGetLastError());
     return ADOCK_OK;
 }
@@ -1062,12 +266,12 @@ extern "C" int adock_eg(const adock_ligands_t* lig, const adock_work_t* work, co
     ADOCK_CHECK_ARG(n >= 0, "n must be >= 0");
     if (n == 0) return ADOCK_OK;
     ADOCK_CHECK_ARG(chain_lig && state && e_out && g_out, "null array argument");
-    TypeTables tt = make_tables(sf);
+    const TypeTables tt = make_tables(sf);
     cudaStream_t st = (cudaStream_t)stream;
     switch (grids->dtype) {
-        case ADOCK_GRID_F32: return launch_eg_apl<float>(P, chain_lig, n, state, e_out, g_out, exact, tt, st);
-        case ADOCK_GRID_F16: return launch_eg_apl<__half>(P, chain_lig, n, state, e_out, g_out, exact, tt, st);
-        case ADOCK_GRID_BF16: return launch_eg_apl<__nv_bfloat16>(P, chain_lig, n, state, e_out, g_out, exact, tt, st);
+        case ADOCK_GRID_F32: return launch_eg<float>(P, chain_lig, n, state, e_out, g_out, exact, tt, st);
+        case ADOCK_GRID_F16: return launch_eg<__half>(P, chain_lig, n, state, e_out, g_out, exact, tt, st);
+        case ADOCK_GRID_BF16: return launch_eg<__nv_bfloat16>(P, chain_lig, n, state, e_out, g_out, exact, tt, st);
     }
     ADOCK_CHECK_ARG(false, "unknown grid dtype %d", grids->dtype);
 }
@@ -1086,6 +290,7 @@ extern "C" int adock_mc(const adock_ligands_t* lig, const adock_work_t* work, co
                     "null array argument");
     ADOCK_CHECK_ARG(!mc->nbr || mc->nbr_n, "nbr without nbr_n");
     ADOCK_CHECK_ARG(mc->temp > 0.f, "temperature must be > 0");
+    ADOCK_CHECK_ARG(mc->variant >= 0 && mc->variant < 4, "variant must be in [0, 3]");
     McParams M;
     M.chain_lig = mc->chain_lig; M.chain_id = mc->chain_id; M.n_chains = mc->n_chains;
     M.nbr = mc->nbr; M.nbr_n = mc->nbr_n; M.nb_max = mc->nb_max;
@@ -1093,13 +298,12 @@ extern "C" int adock_mc(const adock_ligands_t* lig, const adock_work_t* work, co
     M.init_opt = mc->init_opt; M.mc_steps = mc->mc_steps; M.bfgs_iters = mc->bfgs_iters;
     M.temp = mc->temp; M.amp_pos = mc->amp_pos; M.amp_rot = mc->amp_rot; M.seed = mc->seed;
     M.step_offset = mc->step_offset; M.exact = mc->exact; M.order = mc->order; M.queue = mc->queue; M.evals = mc->evals;
-    TypeTables tt = make_tables(sf);
+    const TypeTables tt = make_tables(sf);
     cudaStream_t st = (cudaStream_t)stream;
-    const int wpb = 4;
     switch (grids->dtype) {
-        case ADOCK_GRID_F32: return launch_mc_apl<float>(P, M, tt, st, wpb);
-        case ADOCK_GRID_F16: return launch_mc_apl<__half>(P, M, tt, st, wpb);
-        case ADOCK_GRID_BF16: return launch_mc_apl<__nv_bfloat16>(P, M, tt, st, wpb);
+        case ADOCK_GRID_F32: return launch_mc<float>(P, M, tt, st, mc->variant);
+        case ADOCK_GRID_F16: return launch_mc<__half>(P, M, tt, st, mc->variant);
+        case ADOCK_GRID_BF16: return launch_mc<__nv_bfloat16>(P, M, tt, st, mc->variant);
     }
     ADOCK_CHECK_ARG(false, "unknown grid dtype %d", grids->dtype);
 }
@@ -1116,25 +320,17 @@ extern "C" int adock_stage_a(const adock_ligands_t* lig, const adock_work_t* wor
     ADOCK_CHECK_ARG(conf && quats && trans && ntrans && best_e && best_i, "null array argument");
     const long long blocks = (long long)lig->L * C * Q;
     ADOCK_CHECK_ARG(blocks < (1LL << 31), "too many Stage-A blocks");
-    const size_t smem = (size_t)P.AM * sizeof(float4);
     cudaStream_t st = (cudaStream_t)stream;
     switch (grids->dtype) {
         case ADOCK_GRID_F32:
-            stage_a_kernel<float><<<(unsigned)blocks, 256, smem, st>>>(P, conf, C, quats, Q, trans, ntrans, nt_max, cap,
-                                                                        best_e, best_i);
-            break;
+            return launch_stage_a<float>(P, blocks, conf, C, quats, Q, trans, ntrans, nt_max, cap, best_e, best_i, st);
         case ADOCK_GRID_F16:
-            stage_a_kernel<__half><<<(unsigned)blocks, 256, smem, st>>>(P, conf, C, quats, Q, trans, ntrans, nt_max, cap,
-                                                                         best_e, best_i);
-            break;
+            return launch_stage_a<__half>(P, blocks, conf, C, quats, Q, trans, ntrans, nt_max, cap, best_e, best_i, st);
         case ADOCK_GRID_BF16:
-            stage_a_kernel<__nv_bfloat16><<<(unsigned)blocks, 256, smem, st>>>(P, conf, C, quats, Q, trans, ntrans, nt_max,
-                                                                                cap, best_e, best_i);
-            break;
-        default: ADOCK_CHECK_ARG(false, "unknown grid dtype %d", grids->dtype);
+            return launch_stage_a<__nv_bfloat16>(P, blocks, conf, C, quats, Q, trans, ntrans, nt_max, cap, best_e,
+                                                 best_i, st);
     }
-    ADOCK_CUDA(cudaGetLastError());
-    return ADOCK_OK;
+    ADOCK_CHECK_ARG(false, "unknown grid dtype %d", grids->dtype);
 }
 
 extern "C" int adock_neighbours(const adock_ligands_t* lig, const adock_work_t* work, const adock_sf_t* sf,
@@ -1164,27 +360,16 @@ extern "C" int adock_rescore64(const adock_ligands_t* lig, const adock_work_t* w
     if (n == 0) return ADOCK_OK;
     ADOCK_CHECK_ARG(chain_lig && state && e_total && e_intra && X, "null array argument");
     ADOCK_CHECK_ARG(P.rxyz || (grids && grids->flat), "grids or receptor atoms are required");
-    TypeTables tt = make_tables(sf);
-    const int wpb = 4;
-    const size_t smem = (size_t)wpb * P.AM * 3 * sizeof(double);
-    const unsigned blocks = (unsigned)((n + wpb - 1) / wpb);
+    const TypeTables tt = make_tables(sf);
     cudaStream_t st = (cudaStream_t)stream;
     const int dt = grids ? grids->dtype : ADOCK_GRID_F32;
     switch (dt) {
-        case ADOCK_GRID_F32:
-            rescore64_kernel<float><<<blocks, 32 * wpb, smem, st>>>(P, chain_lig, n, state, e_total, e_intra, X, tt, *sf);
-            break;
-        case ADOCK_GRID_F16:
-            rescore64_kernel<__half><<<blocks, 32 * wpb, smem, st>>>(P, chain_lig, n, state, e_total, e_intra, X, tt, *sf);
-            break;
+        case ADOCK_GRID_F32: return launch_rescore64<float>(P, chain_lig, n, state, e_total, e_intra, X, tt, *sf, st);
+        case ADOCK_GRID_F16: return launch_rescore64<__half>(P, chain_lig, n, state, e_total, e_intra, X, tt, *sf, st);
         case ADOCK_GRID_BF16:
-            rescore64_kernel<__nv_bfloat16><<<blocks, 32 * wpb, smem, st>>>(P, chain_lig, n, state, e_total, e_intra, X,
-                                                                             tt, *sf);
-            break;
-        default: ADOCK_CHECK_ARG(false, "unknown grid dtype %d", dt);
+            return launch_rescore64<__nv_bfloat16>(P, chain_lig, n, state, e_total, e_intra, X, tt, *sf, st);
     }
-    ADOCK_CUDA(cudaGetLastError());
-    return ADOCK_OK;
+    ADOCK_CHECK_ARG(false, "unknown grid dtype %d", dt);
 }
 
 // ------------------------------------------------------------------------------------------ no-allocation MC
@@ -1227,7 +412,7 @@ static int noalloc_scratch(void** out) {
 extern "C" size_t adock_mc_noalloc_scratch_bytes(int L, int AM, int KM, int P) {
     using adock::round256;
     return round256(sizeof(int)) + round256((size_t)L * AM * 16) + round256((size_t)L * AM * 4) +
-           round256((size_t)L * KM * 32) + round256((size_t)L * P * 8) + round256((size_t)L * 16) +
+           round256((size_t)L * KM * 32) + round256((size_t)L * pad32(P) * 8) + round256((size_t)L * 16) +
            round256((size_t)L * 4);
 }
 
@@ -1249,7 +434,7 @@ extern "C" int adock_mc_noalloc(const adock_ligands_t* lig, const adock_grids_t*
     work.atoms = p; p += round256((size_t)lig->L * lig->AM * 16);
     work.masks = p; p += round256((size_t)lig->L * lig->AM * 4);
     work.tors = p;  p += round256((size_t)lig->L * lig->KM * 32);
-    work.pairs = p; p += round256((size_t)lig->L * lig->P * 8);
+    work.pairs = p; p += round256((size_t)lig->L * pad32(lig->P) * 8);
     work.info = p;  p += round256((size_t)lig->L * 16);
     work.rg = p;
     rc = adock_prepare(lig, sf, &work, stream);

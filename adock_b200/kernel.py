@@ -77,7 +77,7 @@ class B200KernelProblem:
         self.t_work = [torch.empty(L * AM * 4, dtype=torch.float32, device=dev),
                        torch.empty(L * AM, dtype=torch.int32, device=dev),
                        torch.empty(L * KM * 2 * 4, dtype=torch.float32, device=dev),
-                       torch.empty(L * self.P * 2, dtype=torch.int32, device=dev),
+                       torch.empty(L * (-(-self.P // 32) * 32) * 2, dtype=torch.int32, device=dev),
                        torch.empty(L * 4, dtype=torch.int32, device=dev),
                        torch.empty(L, dtype=torch.float32, device=dev)]
         w = _lib.Work()
@@ -132,10 +132,17 @@ class B200KernelProblem:
             self._cost = (25 + na) / 3 * (na + npr / 16 + 8)
         return torch.argsort(-self._cost[cl], stable=True).to(torch.int32)
 
+    def tune(self, chain_lig, state):
+        """Pick the MC launch variant for this batch with the autotuner (cached per shape and device)."""
+        from .autotune import tune_mc
+        self.mc_variant = tune_mc(self, self._i32(chain_lig), state.contiguous())
+        return self.mc_variant
+
     def run_mc(self, chain_lig, chain_id, cur, cur_e, best, best_e, init_opt, mc_steps, bfgs_iters, temp,
-               amp_pos, amp_rot, seed, step_offset, exact=False, nbr=None, nbr_n=None, order=None):
+               amp_pos, amp_rot, seed, step_offset, exact=False, nbr=None, nbr_n=None, order=None, variant=None):
         """In place on cur/cur_e/best/best_e (float32 contiguous CUDA tensors). exact=True with nbr [N, NB] int32 /
-        nbr_n [N]: each chain's exact inter energy loops only over its receptor-atom neighbour list."""
+        nbr_n [N]: each chain's exact inter energy loops only over its receptor-atom neighbour list.
+        variant: MC launch variant (default: the tuned one, else the library default)."""
         N = cur.shape[0]
         if N == 0:
             return
@@ -162,6 +169,7 @@ class B200KernelProblem:
         a.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
         a.step_offset, a.exact = int(step_offset), int(exact)
         a.order, a.queue, a.evals = _lib.ptr(order), _lib.ptr(self.queue), _lib.ptr(self.evals)
+        a.variant = int(getattr(self, "mc_variant", 0) if variant is None else variant)
         with torch.cuda.device(self.device):
             _lib.call("adock_mc", self.c_lig, self.c_work, self.c_grids, self.c_sf, self.c_rec, a, _lib.stream_ptr())
         self._keep_mc = keep

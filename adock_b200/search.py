@@ -158,6 +158,8 @@ def dock_problem_kernel(prob, boxes_c, boxes_s, cfg, seed=0, log=None, stats=Non
     best_e = torch.full((N,), float("inf"), device=dev)
     chain_lig = torch.arange(L, device=dev, dtype=torch.int32).repeat_interleave(M)
     chain_id = torch.arange(N, device=dev, dtype=torch.int32)
+    if cfg.get("autotune", True) and hasattr(kp, "tune") and cfg["mc_steps"] > 0:
+        kp.tune(chain_lig, cur)
     seg = max(1, cfg.get("mc_segment", cfg["mc_steps"]))
     n_seg = max(1, math.ceil(cfg["mc_steps"] / seg)) if cfg["mc_steps"] > 0 else 0
     active = torch.ones(L, dtype=torch.bool, device=dev)

@@ -45,6 +45,7 @@ def _args():
     ap.add_argument("--mc-steps", type=int, default=MC_STEPS)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the map-builder / map-precision section")
     return ap.parse_args()
 
 
@@ -305,10 +306,56 @@ def run_ours(args, rank, world, local_rank):
            "config": {"workload": WORKLOAD, "ligands_per_gpu": args.ligands, "chains": CHAINS, "mc_steps": args.mc_steps,
                       "l2": "flushed (256 MB write) between timed steps", "parallelism": f"ligand shards x{world}"},
            "evals_per_s": evals * world / mc_s, "mc_share_of_step": sum(mc_ms) / sum(step_ms),
-           "roofline": roof, "clocks": clk, "gpu_launches": launches, "e2e": e2e}
+           "roofline": roof, "clocks": clk, "gpu_launches": launches, "e2e": e2e,
+           "mc_autotune": __import__("adock_b200.autotune", fromlist=["cached"]).cached()}
+    if rank == 0 and world == 1 and not args.no_extras:
+        out["grid_and_precision"] = _grid_and_precision(dev, ligs)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = _cpu_baseline(ligs, rec, cfg)
     return out
+
+
+def _grid_and_precision(dev, ligs):
+    """Map builder and map-precision figures on the 8,000-atom receptor (30 A box, 81^3): Vina maps for the 8
+    ligand types and the fitted function's maps, timed with CUDA events; per-pose error of FP32/FP16/BF16 maps
+    against float64 evaluation on 100k random poses of this batch's ligands."""
+    import numpy as np
+    import torch
+    from scipy.spatial import cKDTree
+    from adock_b200 import params, synth
+    from adock_b200.grid import build_grid, build_grid_fit, grid_dims
+    from adock_b200.precision import precision_report
+    rec2 = synth.config_receptor(2)
+    sfp = params.sf_params("vina")
+    o = rec2["center"] - rec2["size"] / 2
+    n = grid_dims(rec2["size"], params.GRID_SPACING)
+    lt = np.unique(np.concatenate([[0]] + [l.types for l in ligs]))
+    spec = params.fitted_spec()
+    pot = params.FittedPotential(spec, params.fitted_weights(), lt)
+    rext = params.receptor_ext_types(rec2["rec_xyz"], rec2["rec_types"], spec)
+
+    def timed(fn, reps=5):
+        fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / reps
+
+    ms_vina = timed(lambda: build_grid(rec2["rec_xyz"], rec2["rec_types"], sfp, o, params.GRID_SPACING, n, lt, device=dev))
+    ms_fit = timed(lambda: build_grid_fit(rec2["rec_xyz"], rext, pot, o, params.GRID_SPACING, n, device=dev))
+    # (point, receptor atom) pairs within the 8 A cutoff: the builder's algorithmic work per type
+    axes = [o[d] + params.GRID_SPACING * np.arange(n[d]) for d in range(3)]
+    pts = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, 3)
+    pairs = int(cKDTree(rec2["rec_xyz"]).count_neighbors(cKDTree(pts), 8.0 - 1e-6))
+    pte = pairs * len(lt)
+    return {"receptor": "8000 atoms, 60 A cube; 30 A box, %dx%dx%d points" % tuple(n), "types": len(lt),
+            "vina_ms": ms_vina, "fitted_ms": ms_fit, "point_atom_pairs": pairs,
+            "vina_pair_type_evals_per_s": pte / (ms_vina / 1e3), "fitted_pair_type_evals_per_s": pte / (ms_fit / 1e3),
+            "precision_100k_poses": precision_report(rec2, ligs, 100_000, device=dev)}
 
 
 def _cpu_baseline(ligs, rec, cfg):

@@ -90,7 +90,8 @@ typedef struct {
     void* atoms;               /* [L, AM] float4: ref xyz + (gslot | typ << 16) bits */
     void* masks;               /* [L, AM] uint32 torsion bitmask of each atom (KM <= 32) */
     void* tors;                /* [L, KM, 2] float4: axp + ax0 bits, axu + ax1 bits */
-    void* pairs;               /* [L, P] int2: (i | j << 8 | flags << 16, radius-sum bits) */
+    void* pairs;               /* [L, ceil(P/32)*32] int2: (i | j << 8 | flags << 16, radius-sum bits), scheduled
+                                  in rounds of 32 with no atom twice per round where possible; empty slots -1 */
     void* info;                /* [L] int4: na, nt, np, rec_idx */
     void* rg;                  /* [L] float */
 } adock_work_t;
@@ -112,6 +113,7 @@ typedef struct {
     const int* order;          /* dev [N] processing order (longest first) or NULL */
     int* queue;                /* dev, 1 int work counter, zeroed by the call on `stream` */
     unsigned long long* evals; /* dev, 2 counters (accumulated): energy evaluations, atom evaluations; or NULL */
+    int variant;               /* launch variant (0 = default; 1-3 = 4, 6, 8 resident blocks per SM), autotuned */
 } adock_mc_args_t;
 
 /* ------------------------------------------------------------------------------------------------ misc */
@@ -138,7 +140,8 @@ int adock_grid_fit(const float* rec_xyz, const int* rec_ext, int n_rec, const fl
                    const float* rad_lig, int n_lt, const float* W, float ox, float oy, float oz, float spacing,
                    int nx, int ny, int nz, const float* prm, float* out, void* stream);
 
-/* Down-convert FP32 maps to FP16 (dtype ADOCK_GRID_F16) or BF16 (ADOCK_GRID_BF16), round to nearest. */
+/* Down-convert FP32 maps to FP16 (dtype ADOCK_GRID_F16, saturating at +-65504) or BF16 (ADOCK_GRID_BF16), round
+ * to nearest. No reference counterpart (the reference stores FP32 maps only). */
 int adock_grid_convert(const float* src, void* dst, long long n, int dtype, void* stream);
 
 /* ------------------------------------------------------------------------------------------------ search */

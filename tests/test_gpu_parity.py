@@ -249,3 +249,35 @@ def test_rescore64_matches_torch_fp64(dev):
     want_t = (inter + pen + intra).reshape(-1).numpy()
     assert rel_close(et.cpu().numpy(), want_t, 1e-5, 1e-5) < 1e-5
     assert rel_close(ei.cpu().numpy(), intra.reshape(-1).numpy(), 1e-5, 1e-5) < 1e-5
+
+
+@pytest.mark.parametrize("kind", ["mixed", "big"])
+def test_pair_schedule_is_a_permutation_with_few_repeats(dev, kind):
+    """adock_prepare reorders each ligand's intra pairs into rounds of 32: every pair exactly once, empty slots
+    marked, and within a round an atom appears at most about the unavoidable ceil(64 / na) times."""
+    from adock_b200.kernel import B200KernelProblem
+    pg, pc = _problems(dev, kind=kind)
+    kp = B200KernelProblem(pg)
+    torch.cuda.synchronize()
+    P_pad = -(-kp.P // 32) * 32
+    sched = kp.t_work[3].view(pc.lb.L, P_pad, 2).cpu().numpy()
+    for l, p in enumerate(pc.lb.preps):
+        if len(p.pairs) == 0:
+            assert (sched[l, :, 0] < 0).all()
+            continue
+        rec = sched[l, :, 0]
+        valid = rec >= 0
+        got = sorted(zip((rec[valid] & 0xff).tolist(), ((rec[valid] >> 8) & 0xff).tolist()))
+        hv = np.where(p.heavy)[0]
+        remap = {int(a): i for i, a in enumerate(hv)}
+        want = sorted((remap[int(i)], remap[int(j)]) for i, j in p.pairs)
+        assert got == want
+        R = -(-len(p.pairs) // 32)
+        assert not valid[R * 32:].any()
+        mult = []
+        for r in range(R):
+            rr = rec[r * 32:(r + 1) * 32]
+            rr = rr[rr >= 0]
+            mult.append(np.bincount(np.concatenate([rr & 0xff, (rr >> 8) & 0xff])).max())
+        bound = -(-64 // p.n)
+        assert np.mean(mult) <= bound + 1.5 and max(mult) <= bound + 3, (np.mean(mult), max(mult), bound)
