@@ -32,7 +32,7 @@ class Ligands(ctypes.Structure):
 
 class Grids(ctypes.Structure):
     _fields_ = [("flat", P), ("offs", P), ("dims", P), ("origin", P), ("lo", P), ("hi", P), ("R", I),
-                ("dtype", I), ("spacing", F), ("penalty", F)]
+                ("dtype", I), ("spacing", F), ("penalty", F), ("nmaps", P)]
 
 
 class Receptors(ctypes.Structure):
@@ -47,7 +47,9 @@ class McArgs(ctypes.Structure):
     _fields_ = [("chain_lig", P), ("chain_id", P), ("n_chains", I), ("nbr", P), ("nbr_n", P), ("nb_max", I),
                 ("cur", P), ("cur_e", P), ("best", P), ("best_e", P), ("init_opt", I), ("mc_steps", I),
                 ("bfgs_iters", I), ("temp", F), ("amp_pos", F), ("amp_rot", F), ("seed", ctypes.c_ulonglong),
-                ("step_offset", I), ("exact", I), ("order", P), ("queue", P), ("evals", P), ("variant", I)]
+                ("step_offset", I), ("exact", I), ("order", P), ("queue", P), ("evals", P), ("variant", I),
+                ("prop", P), ("prop_k", I), ("prop_stats", P), ("log_x", P), ("log_y", P), ("log_n", P),
+                ("log_cap", I)]
 
 
 SP = ctypes.POINTER
@@ -65,6 +67,15 @@ _SIGS = {
     "adock_rescore64": ([SP(Ligands), SP(Work), SP(Grids), SP(SF), SP(Receptors), P, I, P, P, P, P, P], I),
     "adock_mc_noalloc_scratch_bytes": ([I, I, I, I], ctypes.c_size_t),
     "adock_mc_noalloc": ([SP(Ligands), SP(Grids), SP(SF), SP(Receptors), SP(McArgs), P], I),
+    "adock_prop_features": ([SP(Ligands), SP(Work), SP(Grids), SP(SF), P, I, P, P, P], I),
+    "adock_prop_sample": ([SP(Ligands), SP(Work), P, P, I, P, I, ctypes.c_ulonglong, I, P, P], I),
+    "adock_gemm_bf16": ([I, I, I, P, ctypes.c_longlong, ctypes.c_longlong, P, ctypes.c_longlong, ctypes.c_longlong, P,
+                         ctypes.c_longlong, F, P, I, P, P, ctypes.c_longlong, P], I),
+    "adock_mlp_nll": ([P, P, I, P, P, P], I),
+    "adock_silu_backward": ([P, P, ctypes.c_longlong, P, P], I),
+    "adock_bias_grad": ([P, I, I, P, P], I),
+    "adock_adam": ([P, P, P, P, P, ctypes.c_longlong, F, F, F, F, I, F, P], I),
+    "adock_f32_to_bf16": ([P, P, ctypes.c_longlong, P], I),
 }
 EXPORTS = tuple(_SIGS)
 

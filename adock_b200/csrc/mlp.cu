@@ -1,0 +1,265 @@
+// Proposal network kernels (sm_100a): BF16 GEMM on the tensor cores with FP32 accumulation and fused epilogues,
+// Gaussian negative log-likelihood + its gradient, SiLU backward, bias-gradient reduction, Adam.
+//
+// Network: x [288] -> SiLU(W1 x + b1) [256] -> SiLU(W2 h1 + b2) [256] -> W3 h2 + b3 [64]. Output columns 0..25 are
+// the means and 32..57 the log standard deviations of the move (translation 3, rotation vector 3, torsions 20).
+//
+// GEMM: C[M,N] = A[M,K] B[K,N] with A and B in BF16 at arbitrary (row, column) strides, so the same kernel serves
+// the forward pass (X W), the input gradient (dY W^T) and the weight gradient (X^T dY). 64x64 CTA tile, 4 warps of
+// 32x32, K step 32, mma.m16n8k16 BF16 -> FP32.
+#include "common.cuh"
+
+namespace adock {
+
+#define GM 64
+#define GN 64
+#define GK 32
+#define APAD 8
+
+struct GemmArgs {
+    int M, N, K;
+    const __nv_bfloat16* A;
+    long long sAm, sAk;
+    const __nv_bfloat16* B;
+    long long sBk, sBn;
+    // epilogue
+    float* C;             // FP32 output [M, ldc] (optional)
+    long long ldc;
+    float beta;           // C = acc + beta * C
+    const float* bias;    // [N] (optional)
+    int act;              // 0 none, 1 SiLU
+    float* pre;           // FP32 pre-activation copy [M, ldc] (optional)
+    __nv_bfloat16* Cb;    // BF16 output [M, ldcb] (optional)
+    long long ldcb;
+};
+
+__device__ __forceinline__ float silu(float x) { return x / (1.f + __expf(-x)); }
+
+__device__ __forceinline__ void mma_bf16(float* d, const uint32_t* a, const uint32_t* b) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__global__ void __launch_bounds__(128) gemm_bf16_kernel(const __grid_constant__ GemmArgs g) {
+    __shared__ __align__(16) __nv_bfloat16 As[GM][GK + APAD];   // [m][k]
+    __shared__ __align__(16) __nv_bfloat16 Bs[GN][GK + APAD];   // [n][k] (transposed: k contiguous)
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int m0 = blockIdx.y * GM, n0 = blockIdx.x * GN;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    const int gid = lane >> 2, tig = lane & 3;
+    float acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.f;
+    const bool a_kfast = g.sAk == 1, b_kfast = g.sBk == 1;
+    const __nv_bfloat16 zero = __float2bfloat16(0.f);
+    for (int k0 = 0; k0 < g.K; k0 += GK) {
+        // stage A[m0:m0+64, k0:k0+32] and B[k0:k0+32, n0:n0+64]; the contiguous dimension runs across threads
+        for (int e = tid; e < GM * GK; e += 128) {
+            const int mm = a_kfast ? e / GK : e % GM, kk = a_kfast ? e % GK : e / GM;
+            const int m = m0 + mm, k = k0 + kk;
+            As[mm][kk] = (m < g.M && k < g.K) ? g.A[(long long)m * g.sAm + (long long)k * g.sAk] : zero;
+        }
+        for (int e = tid; e < GN * GK; e += 128) {
+            const int nn = b_kfast ? e / GK : e % GN, kk = b_kfast ? e % GK : e / GN;
+            const int n = n0 + nn, k = k0 + kk;
+            Bs[nn][kk] = (n < g.N && k < g.K) ? g.B[(long long)k * g.sBk + (long long)n * g.sBn] : zero;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int ks = 0; ks < GK; ks += 16) {
+            uint32_t af[2][4], bf[4][2];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const int r = wm + i * 16 + gid;
+                af[i][0] = *(const uint32_t*)&As[r][ks + tig * 2];
+                af[i][1] = *(const uint32_t*)&As[r + 8][ks + tig * 2];
+                af[i][2] = *(const uint32_t*)&As[r][ks + tig * 2 + 8];
+                af[i][3] = *(const uint32_t*)&As[r + 8][ks + tig * 2 + 8];
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int c = wn + j * 8 + gid;
+                bf[j][0] = *(const uint32_t*)&Bs[c][ks + tig * 2];
+                bf[j][1] = *(const uint32_t*)&Bs[c][ks + tig * 2 + 8];
+            }
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) mma_bf16(acc[i][j], af[i], bf[j]);
+        }
+        __syncthreads();
+    }
+    // epilogue: acc[i][j] = rows (gid, gid + 8), cols (tig * 2, tig * 2 + 1) of tile (i, j)
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int m = m0 + wm + i * 16 + gid + (r >> 1) * 8;
+                const int n = n0 + wn + j * 8 + tig * 2 + (r & 1);
+                if (m >= g.M || n >= g.N) continue;
+                float v = acc[i][j][r];
+                if (g.C && g.beta != 0.f) v += g.beta * g.C[(long long)m * g.ldc + n];
+                if (g.bias) v += g.bias[n];
+                if (g.pre) g.pre[(long long)m * g.ldc + n] = v;
+                if (g.act == 1) v = silu(v);
+                if (g.C) g.C[(long long)m * g.ldc + n] = v;
+                if (g.Cb) g.Cb[(long long)m * g.ldcb + n] = __float2bfloat16(v);
+            }
+}
+
+// Gaussian NLL over the move dimensions: out [B, 64] (mu = out[:, 0:26], log_sigma = out[:, 32:58] clamped to
+// [-4, 2]); target [B, 32] (move in 0..25, torsion count in 26); rows of the batch weighted equally.
+// Writes dOut (BF16, [B, 64]) = d(mean loss)/d(out) and accumulates the loss sum into *loss.
+__global__ void nll_kernel(const float* __restrict__ out, const float* __restrict__ target, int B,
+                           __nv_bfloat16* __restrict__ dout, float* __restrict__ loss) {
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (row >= B) return;
+    const float* o = out + (long long)row * 64;
+    const float* t = target + (long long)row * 32;
+    const int nt = (int)t[26];
+    const float inv = 1.f / (float)B;
+    float l = 0.f, dmu = 0.f, dls = 0.f;
+    const int d = lane;
+    const bool active = d < 26 && (d < 6 || d - 6 < nt);
+    if (active) {
+        const float mu = o[d], ls_raw = o[32 + d];
+        const float ls = fminf(fmaxf(ls_raw, -4.f), 2.f);
+        const float z = (t[d] - mu) * __expf(-ls);
+        l = 0.5f * z * z + ls;
+        dmu = -z * __expf(-ls) * inv;
+        dls = (ls_raw > -4.f && ls_raw < 2.f) ? (1.f - z * z) * inv : 0.f;
+    }
+    dout[(long long)row * 64 + lane] = __float2bfloat16(dmu);
+    dout[(long long)row * 64 + 32 + lane] = __float2bfloat16(dls);
+    l = warp_sum(l);
+    if (lane == 0) atomicAdd(loss, l);
+}
+
+// dA = dH * SiLU'(A) (A = pre-activation FP32), BF16 output
+__global__ void silu_backward_kernel(const float* __restrict__ dH, const float* __restrict__ A, long long n,
+                                     __nv_bfloat16* __restrict__ dA) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float a = A[i];
+        const float s = 1.f / (1.f + __expf(-a));
+        dA[i] = __float2bfloat16(dH[i] * s * (1.f + a * (1.f - s)));
+    }
+}
+
+// db[n] = sum_rows dA[row, n] (BF16 input, FP32 sums); one block per 32 columns
+__global__ void bias_grad_kernel(const __nv_bfloat16* __restrict__ dA, int rows, int cols, float* __restrict__ db) {
+    __shared__ float part[8][33];
+    const int c = blockIdx.x * 32 + (threadIdx.x & 31), w = threadIdx.x >> 5;
+    float s = 0.f;
+    if (c < cols)
+        for (int r = w; r < rows; r += 8) s += __bfloat162float(dA[(long long)r * cols + c]);
+    part[w][threadIdx.x & 31] = s;
+    __syncthreads();
+    if (w == 0 && c < cols) {
+        float t = 0.f;
+        for (int i = 0; i < 8; ++i) t += part[i][threadIdx.x & 31];
+        db[c] = t;
+    }
+}
+
+// Adam on FP32 master parameters, refreshing their BF16 copies (bias_hat corrections from the step count)
+__global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ grad, float* __restrict__ m,
+                            float* __restrict__ v, __nv_bfloat16* __restrict__ pb, long long n, float lr, float b1,
+                            float b2, float eps, float c1, float c2, float wd) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float gi = grad[i] + wd * p[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi, vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        const float pi = p[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        p[i] = pi;
+        if (pb) pb[i] = __float2bfloat16(pi);
+    }
+}
+
+__global__ void f32_to_bf16_kernel(const float* __restrict__ x, __nv_bfloat16* __restrict__ y, long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        y[i] = __float2bfloat16(x[i]);
+}
+
+static unsigned grid1d(long long n) {
+    long long b = (n + 255) / 256;
+    const long long cap = 148LL * 32;
+    return (unsigned)(b < 1 ? 1 : (b > cap ? cap : b));
+}
+
+}  // namespace adock
+
+using namespace adock;
+
+extern "C" int adock_gemm_bf16(int M, int N, int K, const void* A, long long sAm, long long sAk, const void* B,
+                               long long sBk, long long sBn, float* C, long long ldc, float beta, const float* bias,
+                               int act, float* pre, void* Cb, long long ldcb, void* stream) {
+    ADOCK_CHECK_ARG(M >= 0 && N >= 0 && K >= 0, "negative GEMM size");
+    if (M == 0 || N == 0) return ADOCK_OK;
+    ADOCK_CHECK_ARG(A && B && (C || Cb), "null GEMM operand");
+    ADOCK_CHECK_ARG(act == 0 || act == 1, "act must be 0 (none) or 1 (SiLU)");
+    ADOCK_CHECK_ARG(!pre || C, "pre-activation output needs C's leading dimension");
+    GemmArgs g;
+    g.M = M; g.N = N; g.K = K;
+    g.A = (const __nv_bfloat16*)A; g.sAm = sAm; g.sAk = sAk;
+    g.B = (const __nv_bfloat16*)B; g.sBk = sBk; g.sBn = sBn;
+    g.C = C; g.ldc = ldc; g.beta = beta; g.bias = bias; g.act = act; g.pre = pre;
+    g.Cb = (__nv_bfloat16*)Cb; g.ldcb = ldcb;
+    dim3 grid((N + GN - 1) / GN, (M + GM - 1) / GM);
+    ADOCK_CHECK_ARG(grid.y < 65536u, "M too large");
+    gemm_bf16_kernel<<<grid, 128, 0, (cudaStream_t)stream>>>(g);
+    ADOCK_CUDA(cudaGetLastError());
+    return ADOCK_OK;
+}
+
+extern "C" int adock_mlp_nll(const float* out, const float* target, int B, void* dout, float* loss, void* stream) {
+    ADOCK_CHECK_ARG(out && target && dout && loss && B >= 0, "bad argument");
+    if (B == 0) return ADOCK_OK;
+    nll_kernel<<<(B + 3) / 4, 128, 0, (cudaStream_t)stream>>>(out, target, B, (__nv_bfloat16*)dout, loss);
+    ADOCK_CUDA(cudaGetLastError());
+    return ADOCK_OK;
+}
+
+extern "C" int adock_silu_backward(const float* dH, const float* A, long long n, void* dA, void* stream) {
+    ADOCK_CHECK_ARG(dH && A && dA && n >= 0, "bad argument");
+    if (n == 0) return ADOCK_OK;
+    silu_backward_kernel<<<grid1d(n), 256, 0, (cudaStream_t)stream>>>(dH, A, n, (__nv_bfloat16*)dA);
+    ADOCK_CUDA(cudaGetLastError());
+    return ADOCK_OK;
+}
+
+extern "C" int adock_bias_grad(const void* dA, int rows, int cols, float* db, void* stream) {
+    ADOCK_CHECK_ARG(dA && db && rows >= 0 && cols >= 0, "bad argument");
+    if (cols == 0) return ADOCK_OK;
+    bias_grad_kernel<<<(cols + 31) / 32, 256, 0, (cudaStream_t)stream>>>((const __nv_bfloat16*)dA, rows, cols, db);
+    ADOCK_CUDA(cudaGetLastError());
+    return ADOCK_OK;
+}
+
+extern "C" int adock_adam(float* p, const float* grad, float* m, float* v, void* pb, long long n, float lr, float b1,
+                          float b2, float eps, int step, float wd, void* stream) {
+    ADOCK_CHECK_ARG(p && grad && m && v && n >= 0 && step >= 1, "bad argument");
+    if (n == 0) return ADOCK_OK;
+    const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
+    adam_kernel<<<grid1d(n), 256, 0, (cudaStream_t)stream>>>(p, grad, m, v, (__nv_bfloat16*)pb, n, lr, b1, b2, eps, c1,
+                                                             c2, wd);
+    ADOCK_CUDA(cudaGetLastError());
+    return ADOCK_OK;
+}
+
+extern "C" int adock_f32_to_bf16(const float* x, void* y, long long n, void* stream) {
+    ADOCK_CHECK_ARG(x && y && n >= 0, "bad argument");
+    if (n == 0) return ADOCK_OK;
+    f32_to_bf16_kernel<<<grid1d(n), 256, 0, (cudaStream_t)stream>>>(x, (__nv_bfloat16*)y, n);
+    ADOCK_CUDA(cudaGetLastError());
+    return ADOCK_OK;
+}

@@ -191,6 +191,30 @@ __global__ void __launch_bounds__(256) neighbours_kernel(const __grid_constant__
     if (threadIdx.x == 0) nbr_n[ch] = base_sh;
 }
 
+// ------------------------------------------------------------------------------------------ proposal sampling
+// moves[c, k, d] = mean[c, d] + exp(clamp(log_sd[c, d], -4, 2)) * z, z ~ N(0, 1) by Box-Muller on the counter-based
+// stream (seed, chain id, 64 * segment + k, 2 d / 2 d + 1); torsion entries past the ligand's count are 0.
+__global__ void prop_sample_kernel(const int4* info, const int* chain_lig, const int* chain_id, int n,
+                                   const float* out, int k, unsigned long long seed, int segment, float* moves) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)n * k * PROP_MOVE) return;
+    const int d = (int)(idx % PROP_MOVE);
+    const int kk = (int)((idx / PROP_MOVE) % k);
+    const int c = (int)(idx / ((long long)PROP_MOVE * k));
+    const int nt = info[chain_lig[c]].y;
+    float v = 0.f;
+    if (d < 26 && (d < 6 || d - 6 < nt)) {
+        const int cid = chain_id[c], step = 64 * segment + kk;
+        const float u1 = fmaxf(uniform01(seed, cid, step, 2 * d), 1e-7f);
+        const float u2 = uniform01(seed, cid, step, 2 * d + 1);
+        const float z = sqrtf(-2.f * __logf(u1)) * __cosf(6.28318531f * u2);
+        const float mu = out[(long long)c * 64 + d];
+        const float ls = fminf(fmaxf(out[(long long)c * 64 + 32 + d], -4.f), 2.f);
+        v = mu + __expf(ls) * z;
+    }
+    moves[idx] = v;
+}
+
 // ------------------------------------------------------------------------------------------ host side
 static TypeTables make_tables(const adock_sf_t* sf) {
     TypeTables t;
@@ -219,9 +243,11 @@ static int make_params(SearchParams& P, const adock_ligands_t* lig, const adock_
         P.flat = grids->flat; P.offs = grids->offs; P.dims = grids->dims;
         P.origin = grids->origin; P.lo = grids->lo; P.hi = grids->hi;
         P.inv_s = 1.f / grids->spacing; P.pen = grids->penalty;
+        P.nmaps = grids->nmaps;
     } else {
         P.flat = nullptr; P.offs = nullptr; P.dims = nullptr; P.origin = P.lo = P.hi = nullptr;
         P.inv_s = 1.f; P.pen = 0.f;
+        P.nmaps = nullptr;
     }
     if (rec && rec->xyz) {
         P.rxyz = rec->xyz; P.rtyp = rec->typ; P.rn = rec->n; P.RN = rec->RN;
@@ -298,6 +324,10 @@ extern "C" int adock_mc(const adock_ligands_t* lig, const adock_work_t* work, co
     M.init_opt = mc->init_opt; M.mc_steps = mc->mc_steps; M.bfgs_iters = mc->bfgs_iters;
     M.temp = mc->temp; M.amp_pos = mc->amp_pos; M.amp_rot = mc->amp_rot; M.seed = mc->seed;
     M.step_offset = mc->step_offset; M.exact = mc->exact; M.order = mc->order; M.queue = mc->queue; M.evals = mc->evals;
+    ADOCK_CHECK_ARG(!mc->prop || mc->prop_k >= 1, "prop_k must be >= 1 with proposals");
+    ADOCK_CHECK_ARG(!mc->log_x || (mc->log_y && mc->log_n && mc->log_cap >= 0), "incomplete training-data log");
+    M.prop = mc->prop; M.prop_k = mc->prop_k; M.prop_stats = mc->prop_stats;
+    M.log_x = (__nv_bfloat16*)mc->log_x; M.log_y = mc->log_y; M.log_n = mc->log_n; M.log_cap = mc->log_cap;
     const TypeTables tt = make_tables(sf);
     cudaStream_t st = (cudaStream_t)stream;
     switch (grids->dtype) {
@@ -442,4 +472,40 @@ extern "C" int adock_mc_noalloc(const adock_ligands_t* lig, const adock_grids_t*
     adock_mc_args_t m = *mc;
     m.queue = queue;   // adock_mc clears the counter on `stream` before its launch
     return adock_mc(lig, &work, grids, sf, rec, &m, stream);
+}
+
+// ------------------------------------------------------------------------------------------ proposal entry points
+extern "C" int adock_prop_features(const adock_ligands_t* lig, const adock_work_t* work, const adock_grids_t* grids,
+                                   const adock_sf_t* sf, const int* chain_lig, int n, const float* state, void* feat,
+                                   void* stream) {
+    SearchParams P;
+    int rc = make_params(P, lig, work, grids, sf, nullptr);
+    if (rc) return rc;
+    ADOCK_CHECK_ARG(grids && grids->flat, "grids are required");
+    ADOCK_CHECK_ARG(n >= 0, "n must be >= 0");
+    if (n == 0) return ADOCK_OK;
+    ADOCK_CHECK_ARG(chain_lig && state && feat, "null array argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    __nv_bfloat16* out = (__nv_bfloat16*)feat;
+    switch (grids->dtype) {
+        case ADOCK_GRID_F32: return launch_prop_features<float>(P, chain_lig, n, state, out, st);
+        case ADOCK_GRID_F16: return launch_prop_features<__half>(P, chain_lig, n, state, out, st);
+        case ADOCK_GRID_BF16: return launch_prop_features<__nv_bfloat16>(P, chain_lig, n, state, out, st);
+    }
+    ADOCK_CHECK_ARG(false, "unknown grid dtype %d", grids->dtype);
+}
+
+extern "C" int adock_prop_sample(const adock_ligands_t* lig, const adock_work_t* work, const int* chain_lig,
+                                 const int* chain_id, int n, const float* net_out, int k, unsigned long long seed,
+                                 int segment, float* moves, void* stream) {
+    ADOCK_CHECK_ARG(lig && work && work->info, "null argument");
+    ADOCK_CHECK_ARG(n >= 0 && k >= 1, "n must be >= 0 and k >= 1");
+    if (n == 0) return ADOCK_OK;
+    ADOCK_CHECK_ARG(chain_lig && chain_id && net_out && moves, "null array argument");
+    const long long total = (long long)n * k * PROP_MOVE;
+    const unsigned blocks = (unsigned)((total + 255) / 256);
+    prop_sample_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>((const int4*)work->info, chain_lig, chain_id, n, net_out,
+                                                                 k, seed, segment, moves);
+    ADOCK_CUDA(cudaGetLastError());
+    return ADOCK_OK;
 }

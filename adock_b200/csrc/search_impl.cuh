@@ -30,6 +30,7 @@ struct SearchParams {
     const float* origin;
     const float* lo;
     const float* hi;
+    const int* nmaps;      // [R] maps built per receptor (may be NULL)
     float inv_s, pen;
     // receptor atoms for exact mode
     const float* rxyz;
@@ -65,7 +66,20 @@ struct McParams {
     const int* order;
     int* queue;
     unsigned long long* evals;
+    // learned proposal: moves [N, prop_k, 32] for steps 0..prop_k-1 of this launch (NULL: plain MC only)
+    const float* prop;
+    int prop_k;
+    unsigned long long* prop_stats;  // [4] proposals made, proposals accepted, plain steps, plain accepted
+    // training-data log of accepted improving moves: features [cap, 288] BF16, moves [cap, 32]
+    __nv_bfloat16* log_x;
+    float* log_y;
+    int* log_n;
+    int log_cap;
 };
+
+#define PROP_IN 288
+#define PROP_MOVE 32
+#define PROP_FAIL_MAX 8
 
 __device__ __forceinline__ int hb_pair(int fa, int fb) {
     return (((fa & 2) && (fb & 4)) || ((fa & 4) && (fb & 2))) ? PF_HB : 0;
@@ -240,7 +254,7 @@ __device__ __forceinline__ float pair_slot(int2 pr, const float4* X, float4* FF,
 // pairs. Gradient: dE/dt = sum F, torque = sum (X - t) x F, dE/dtheta_k = u_k . sum_{a moved by k} (X_a - p_k) x F_a,
 // evaluated as u_k . (sum X' x F - p'_k x sum F) over the subtree of k (X' = X - t).
 template <int APL, typename GT>
-__device__ float eval_eg(float* ws, const WSLayout& L, const float* s, float* g, const Chain<APL>& c,
+__device__ __forceinline__ float eval_eg(float* ws, const WSLayout& L, const float* s, float* g, const Chain<APL>& c,
                          const SearchParams& P, const TypeTables& tt, int lane) {
     float4* X = (float4*)(ws + L.X);
     float4* FF = (float4*)(ws + L.FF);
@@ -450,9 +464,13 @@ __device__ __forceinline__ void neg_hv(const float* H, const float* v, float* ou
 
 // Vina-1.2-style BFGS on state x (shared, in/out); returns the final energy (mckernel.py:267-326).
 // The curvature scalar y.p and the update guard alpha * y.p >= eps are evaluated in float64.
+// Not inlined: the MC kernel calls it from two sites (start optimisation and every step); one copy, with one
+// inlined eval_eg, keeps the kernel small enough for the instruction cache (instruction-fetch stalls were the
+// largest stall reason with four inlined copies of eval_eg).
 template <int APL, typename GT>
-__device__ float bfgs(float* ws, const WSLayout& L, float* x, int iters, const Chain<APL>& c, const SearchParams& P,
-                      const TypeTables& tt, int lane, unsigned& n_eval) {
+__device__ __noinline__ float bfgs(float* ws, const WSLayout& L, float* x, int iters, const Chain<APL>& c_in,
+                                   const SearchParams& P, const TypeTables& tt, int lane, unsigned& n_eval) {
+    const Chain<APL> c = c_in;   // registers for the whole optimisation
     const int D = 6 + c.nt, S = 7 + c.nt;
     float* H = ws + L.H;
     float* g = ws + L.g;
@@ -463,28 +481,42 @@ __device__ float bfgs(float* ws, const WSLayout& L, float* x, int iters, const C
     float* mhy = ws + L.mhy;
     float* xn = ws + L.xn;
     float* xo = ws + L.xo;
-    float f0 = eval_eg<APL, GT>(ws, L, x, g, c, P, tt, lane);
-    ++n_eval;
-    const float f_orig = f0;
-    wcopy(xo, x, S, lane);
-    wcopy(go, g, D, lane);
-    for (int i = lane; i < D; i += 32)
-        for (int j = 0; j < D; ++j) H[j * D + i] = (i == j) ? 1.f : 0.f;
-    __syncwarp();
-    for (int step = 0; step < iters; ++step) {
-        neg_hv(H, g, p, D, lane);
-        const float pg = wdot(p, g, D, lane);
-        float alpha = 1.f, f1 = 0.f;
-        for (int trial = 0; trial < 10; ++trial) {
+    // One evaluation per pass of this loop: the start point on the first pass, then the line-search trial points.
+    // Keeping a single call site keeps a single inlined copy of eval_eg in the kernel.
+    float f0 = 0.f, f_orig = 0.f, pg = 0.f, alpha = 1.f;
+    int step = 0, trial = 0;
+    bool first = true;
+    while (true) {
+        const float f = eval_eg<APL, GT>(ws, L, first ? x : xn, first ? g : gn, c, P, tt, lane);
+        ++n_eval;
+        if (first) {
+            first = false;
+            f0 = f_orig = f;
+            wcopy(xo, x, S, lane);
+            wcopy(go, g, D, lane);
+            for (int i = lane; i < D; i += 32)
+                for (int j = 0; j < D; ++j) H[j * D + i] = (i == j) ? 1.f : 0.f;
+            __syncwarp();
+            if (iters <= 0) break;
+            neg_hv(H, g, p, D, lane);
+            pg = wdot(p, g, D, lane);
+            alpha = 1.f;
+            trial = 0;
             conf_step(xn, x, p, alpha, c.nt, lane);
-            f1 = eval_eg<APL, GT>(ws, L, xn, gn, c, P, tt, lane);
-            ++n_eval;
-            if (f1 - f0 < 1e-4f * alpha * pg) break;
+            continue;
+        }
+        // Armijo test (c = 1e-4); up to 10 trials halving alpha. After a 10th failed trial the last point is taken
+        // with alpha already halved, as in the reference's loop.
+        if (!(f - f0 < 1e-4f * alpha * pg)) {
             alpha *= 0.5f;
+            if (++trial < 10) {
+                conf_step(xn, x, p, alpha, c.nt, lane);
+                continue;
+            }
         }
         for (int i = lane; i < D; i += 32) y[i] = gn[i] - g[i];
         __syncwarp();
-        f0 = f1;
+        f0 = f;
         wcopy(x, xn, S, lane);
         const float gg = wdot(gn, gn, D, lane);
         wcopy(g, gn, D, lane);
@@ -500,18 +532,25 @@ __device__ float bfgs(float* ws, const WSLayout& L, float* x, int iters, const C
             }
         }
         const double ayp = (double)alpha * yp;
-        if (ayp < (double)EPSF) continue;
-        for (int i = lane; i < D; i += 32) mhy[i] = 0.f;
-        neg_hv(H, y, mhy, D, lane);
-        const float yhy = -wdot(y, mhy, D, lane);
-        const float r = (float)(1.0 / ayp);
-        const float c2 = alpha * alpha * (r * r * yhy + r);
-        const float ar = alpha * r;
-        for (int i = lane; i < D; i += 32) {
-            const float mi = mhy[i], pi = p[i];
-            for (int j = 0; j < D; ++j) H[j * D + i] += ar * (mi * p[j] + mhy[j] * pi) + c2 * pi * p[j];
+        if (ayp >= (double)EPSF) {
+            for (int i = lane; i < D; i += 32) mhy[i] = 0.f;
+            neg_hv(H, y, mhy, D, lane);
+            const float yhy = -wdot(y, mhy, D, lane);
+            const float r = (float)(1.0 / ayp);
+            const float c2 = alpha * alpha * (r * r * yhy + r);
+            const float ar = alpha * r;
+            for (int i = lane; i < D; i += 32) {
+                const float mi = mhy[i], pi = p[i];
+                for (int j = 0; j < D; ++j) H[j * D + i] += ar * (mi * p[j] + mhy[j] * pi) + c2 * pi * p[j];
+            }
+            __syncwarp();
         }
-        __syncwarp();
+        if (++step >= iters) break;
+        neg_hv(H, g, p, D, lane);
+        pg = wdot(p, g, D, lane);
+        alpha = 1.f;
+        trial = 0;
+        conf_step(xn, x, p, alpha, c.nt, lane);
     }
     if (!(f0 <= f_orig)) {
         f0 = f_orig;
@@ -519,6 +558,91 @@ __device__ float bfgs(float* ws, const WSLayout& L, float* x, int iters, const C
         wcopy(g, go, D, lane);
     }
     return f0;
+}
+
+// ------------------------------------------------------------------------------------------ proposal features
+// Feature row (288 values, BF16) of state s of ligand l, computed by one warp:
+//   [0, 216)   27 samples x 8 maps: nearest-grid map values at the centroid + {-2, 0, 2} A per axis, as
+//              sign(v) log(1 + |v|) (maps beyond the receptor's count are 0)
+//   [216, 219) translation relative to the box centre / 10 A
+//   [219, 223) orientation quaternion, sign chosen so that w >= 0
+//   [223, 263) sin, cos of torsions 0..19 (0 beyond the ligand's torsion count)
+//   [263, 275) heavy atoms / 64, torsions / 20, radius of gyration / 10, intra pairs / 2000, fraction of atoms
+//              per map slot 0..7
+//   [275, 288) 0
+template <typename GT>
+__device__ void prop_features(const SearchParams& P, int l, const float* s, __nv_bfloat16* out, int lane) {
+    const int4 inf = P.info[l];
+    const int na = inf.x, nt = inf.y, np = inf.z, ri = inf.w;
+    const int nx = (int)P.dims[3 * ri], ny = (int)P.dims[3 * ri + 1], nz = (int)P.dims[3 * ri + 2];
+    const long long n3 = (long long)nx * ny * nz;
+    const int nm = P.nmaps ? min(P.nmaps[ri], 8) : 8;
+    const GT* G = (const GT*)P.flat + P.offs[ri];
+    if (lane < 27) {
+        const float px = s[0] + 2.f * (float)(lane % 3 - 1), py = s[1] + 2.f * (float)((lane / 3) % 3 - 1),
+                    pz = s[2] + 2.f * (float)(lane / 9 - 1);
+        const int i = min(max(__float2int_rn((px - P.origin[3 * ri]) * P.inv_s), 0), nx - 1);
+        const int j = min(max(__float2int_rn((py - P.origin[3 * ri + 1]) * P.inv_s), 0), ny - 1);
+        const int k = min(max(__float2int_rn((pz - P.origin[3 * ri + 2]) * P.inv_s), 0), nz - 1);
+        const long long idx = ((long long)i * ny + j) * nz + k;
+        for (int q = 0; q < 8; ++q) {
+            const float v = q < nm ? gload(G + q * n3 + idx) : 0.f;
+            out[lane * 8 + q] = __float2bfloat16(copysignf(log1pf(fabsf(v)), v));
+        }
+    }
+    if (lane == 27) {
+        for (int d = 0; d < 3; ++d)
+            out[216 + d] = __float2bfloat16((s[d] - 0.5f * (P.lo[3 * ri + d] + P.hi[3 * ri + d])) * 0.1f);
+        float qw = s[3], qx = s[4], qy = s[5], qz = s[6];
+        const float nq = rsqrtf(qw * qw + qx * qx + qy * qy + qz * qz) * (qw < 0.f ? -1.f : 1.f);
+        out[219] = __float2bfloat16(qw * nq); out[220] = __float2bfloat16(qx * nq);
+        out[221] = __float2bfloat16(qy * nq); out[222] = __float2bfloat16(qz * nq);
+        out[263] = __float2bfloat16(na / 64.f); out[264] = __float2bfloat16(nt / 20.f);
+        out[265] = __float2bfloat16(P.rg[l] / 10.f); out[266] = __float2bfloat16(np / 2000.f);
+    }
+    if (lane < 20) {
+        float sv = 0.f, cv = 0.f;
+        if (lane < nt) __sincosf(s[7 + lane], &sv, &cv);
+        out[223 + 2 * lane] = __float2bfloat16(sv);
+        out[224 + 2 * lane] = __float2bfloat16(cv);
+    }
+    if (lane >= 24 && lane < 32) {   // fraction of atoms per map slot
+        const int q = lane - 24;
+        int cnt = 0;
+        for (int a = 0; a < na; ++a) cnt += ((__float_as_int(P.atoms[(long long)l * P.AM + a].w) & 0xffff) == q);
+        out[267 + q] = __float2bfloat16(na ? (float)cnt / na : 0.f);
+    }
+    if (lane < 13) out[275 + lane] = __float2bfloat16(0.f);
+    __syncwarp();
+}
+
+// Move from state a to state b (proposal coordinates): translation, rotation vector of q_b q_a^-1, torsion
+// differences wrapped to [-pi, pi); entry 26 holds the torsion count. Lane 0 writes.
+__device__ __forceinline__ void state_move(const float* a, const float* b, int nt, float* y) {
+    y[0] = b[0] - a[0]; y[1] = b[1] - a[1]; y[2] = b[2] - a[2];
+    // r = q_b * conj(q_a)
+    const float aw = a[3], ax = -a[4], ay = -a[5], az = -a[6];
+    const float bw = b[3], bx = b[4], by = b[5], bz = b[6];
+    float w = bw * aw - bx * ax - by * ay - bz * az;
+    float x = bw * ax + bx * aw + by * az - bz * ay;
+    float yv = bw * ay - bx * az + by * aw + bz * ax;
+    float z = bw * az + bx * ay - by * ax + bz * aw;
+    const float nn = rsqrtf(w * w + x * x + yv * yv + z * z) * (w < 0.f ? -1.f : 1.f);
+    w *= nn; x *= nn; yv *= nn; z *= nn;
+    const float sn = sqrtf(x * x + yv * yv + z * z);
+    const float ang = 2.f * atan2f(sn, w);
+    const float k = sn > 1e-7f ? ang / sn : 2.f;
+    y[3] = x * k; y[4] = yv * k; y[5] = z * k;
+    for (int t = 0; t < 20; ++t) {
+        float d = 0.f;
+        if (t < nt) {
+            d = b[7 + t] - a[7 + t];
+            d = d - 6.28318531f * floorf((d + 3.14159265f) / 6.28318531f);
+        }
+        y[6 + t] = d;
+    }
+    y[26] = (float)nt;
+    for (int t = 27; t < 32; ++t) y[t] = 0.f;
 }
 
 template <int APL, typename GT, int MINB>
@@ -566,27 +690,52 @@ __global__ void __launch_bounds__(128, MINB) mc_kernel(const __grid_constant__ S
             eb = ec;
             wcopy(best, cur, S, lane);
         }
+        int prop_fail = 0;
+        unsigned long long n_prop = 0, n_prop_acc = 0, n_plain = 0, n_plain_acc = 0;
         for (int st = 0; st < M.mc_steps; ++st) {
             const int sg = M.step_offset + st;
             wcopy(x, cur, S, lane);
-            const int nm = 2 + c.nt;
-            const int which = min((int)(uniform01(M.seed, cid, sg, 0) * nm), nm - 1);
-            if (lane == 0) {
-                float v[3];
-                if (which == 0) {
-                    unit_ball(M.seed, cid, sg, 10, v);
-                    x[0] += M.amp_pos * v[0]; x[1] += M.amp_pos * v[1]; x[2] += M.amp_pos * v[2];
-                } else if (which == 1) {
-                    unit_ball(M.seed, cid, sg, 10, v);
-                    const float sc = M.amp_rot / fmaxf(c.rg, 1.0f);
-                    quat_apply_rotvec(x + 3, sc * v[0], sc * v[1], sc * v[2]);
-                } else {
-                    x[7 + which - 2] = (2.f * uniform01(M.seed, cid, sg, 1) - 1.f) * 3.14159265f;
+            // learned move while the proposal has not failed PROP_FAIL_MAX times in a row, else plain MC
+            const bool use_prop = M.prop && prop_fail < PROP_FAIL_MAX;
+            if (use_prop) {
+                const float* mv = M.prop + ((long long)ch * M.prop_k + (st % M.prop_k)) * PROP_MOVE;
+                if (lane == 0) {
+                    x[0] += mv[0]; x[1] += mv[1]; x[2] += mv[2];
+                    quat_apply_rotvec(x + 3, mv[3], mv[4], mv[5]);
+                }
+                for (int k = lane; k < c.nt && k < 20; k += 32) x[7 + k] += mv[6 + k];
+            } else {
+                const int nm = 2 + c.nt;
+                const int which = min((int)(uniform01(M.seed, cid, sg, 0) * nm), nm - 1);
+                if (lane == 0) {
+                    float v[3];
+                    if (which == 0) {
+                        unit_ball(M.seed, cid, sg, 10, v);
+                        x[0] += M.amp_pos * v[0]; x[1] += M.amp_pos * v[1]; x[2] += M.amp_pos * v[2];
+                    } else if (which == 1) {
+                        unit_ball(M.seed, cid, sg, 10, v);
+                        const float sc = M.amp_rot / fmaxf(c.rg, 1.0f);
+                        quat_apply_rotvec(x + 3, sc * v[0], sc * v[1], sc * v[2]);
+                    } else {
+                        x[7 + which - 2] = (2.f * uniform01(M.seed, cid, sg, 1) - 1.f) * 3.14159265f;
+                    }
                 }
             }
             __syncwarp();
             const float en = bfgs<APL, GT>(ws, L, x, iters, c, P, tt, lane, n_eval);
             const bool accept = (en < ec) || (uniform01(M.seed, cid, sg, 2) < __expf((ec - en) / M.temp));
+            if (use_prop) { ++n_prop; n_prop_acc += accept; } else { ++n_plain; n_plain_acc += accept; }
+            prop_fail = accept ? 0 : (use_prop ? prop_fail + 1 : prop_fail);
+            if (accept && en < ec && M.log_x) {   // training data: features of the pre-move state + the move
+                int row = 0;
+                if (lane == 0) row = atomicAdd(M.log_n, 1);
+                row = __shfl_sync(0xffffffffu, row, 0);
+                if (row < M.log_cap) {
+                    prop_features<GT>(P, l, cur, M.log_x + (long long)row * PROP_IN, lane);
+                    if (lane == 0) state_move(cur, x, c.nt, M.log_y + (long long)row * PROP_MOVE);
+                }
+                __syncwarp();
+            }
             if (accept) {
                 ec = en;
                 wcopy(cur, x, S, lane);
@@ -595,6 +744,10 @@ __global__ void __launch_bounds__(128, MINB) mc_kernel(const __grid_constant__ S
                     wcopy(best, x, S, lane);
                 }
             }
+        }
+        if (M.prop_stats && lane == 0 && M.mc_steps > 0) {
+            atomicAdd(&M.prop_stats[0], n_prop); atomicAdd(&M.prop_stats[1], n_prop_acc);
+            atomicAdd(&M.prop_stats[2], n_plain); atomicAdd(&M.prop_stats[3], n_plain_acc);
         }
         for (int i = lane; i < S; i += 32) {
             gcur[i] = cur[i];
@@ -840,6 +993,20 @@ __global__ void __launch_bounds__(128) rescore64_kernel(const __grid_constant__ 
     }
 }
 
+// feature rows of n states (one warp per state)
+template <typename GT>
+__global__ void __launch_bounds__(128) prop_features_kernel(const __grid_constant__ SearchParams P, const int* chain_lig,
+                                                            int n, const float* state, __nv_bfloat16* out) {
+    __shared__ float s[4][7 + 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int ch = blockIdx.x * 4 + wid;
+    if (ch >= n) return;
+    const int SDM = 7 + P.KM;
+    for (int i = lane; i < SDM && i < 7 + 32; i += 32) s[wid][i] = state[(long long)ch * SDM + i];
+    __syncwarp();
+    prop_features<GT>(P, chain_lig[ch], s[wid], out + (long long)ch * PROP_IN, lane);
+}
+
 // ------------------------------------------------------------------------------------------ launchers
 // Launch variants of the persistent MC kernel (128 threads per block): minimum resident blocks per SM, which
 // caps registers per thread (4 -> 128, 6 -> 80, 8 -> 64). Variant 0 is the default.
@@ -933,7 +1100,17 @@ int launch_rescore64(const SearchParams& P, const int* cl, int n, const float* s
     return ADOCK_OK;
 }
 
+template <typename GT>
+int launch_prop_features(const SearchParams& P, const int* cl, int n, const float* state, __nv_bfloat16* out,
+                         cudaStream_t st) {
+    prop_features_kernel<GT><<<(unsigned)((n + 3) / 4), 128, 0, st>>>(P, cl, n, state, out);
+    ADOCK_CUDA(cudaGetLastError());
+    return ADOCK_OK;
+}
+
 #define ADOCK_SEARCH_INSTANTIATE(GT)                                                                              \
+    template int launch_prop_features<GT>(const SearchParams&, const int*, int, const float*, __nv_bfloat16*,     \
+                                          cudaStream_t);                                                          \
     template int launch_mc<GT>(const SearchParams&, const McParams&, const TypeTables&, cudaStream_t, int);       \
     template int launch_eg<GT>(const SearchParams&, const int*, int, const float*, float*, float*, int,           \
                                const TypeTables&, cudaStream_t);                                                  \
@@ -943,6 +1120,8 @@ int launch_rescore64(const SearchParams& P, const int* cl, int n, const float* s
                                       float*, const TypeTables&, const adock_sf_t&, cudaStream_t);
 
 #define ADOCK_SEARCH_EXTERN(GT)                                                                                   \
+    extern template int launch_prop_features<GT>(const SearchParams&, const int*, int, const float*,              \
+                                                 __nv_bfloat16*, cudaStream_t);                                   \
     extern template int launch_mc<GT>(const SearchParams&, const McParams&, const TypeTables&, cudaStream_t, int); \
     extern template int launch_eg<GT>(const SearchParams&, const int*, int, const float*, float*, float*, int,    \
                                       const TypeTables&, cudaStream_t);                                           \

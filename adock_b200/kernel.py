@@ -56,9 +56,12 @@ class B200KernelProblem:
         flat, code = gs.storage(grid_dtype)
         self.t_grid = [flat, gs.offs.to(dev, torch.int64).contiguous(), gs.dims.to(dev, torch.int64).contiguous(),
                        gs.origin.float().contiguous(), gs.lo.float().contiguous(), gs.hi.float().contiguous()]
+        sizes = torch.diff(self.t_grid[1], append=torch.tensor([flat.numel()], device=dev))
+        self.t_nmaps = (sizes // self.t_grid[2].prod(1)).to(torch.int32).contiguous()
         g = _lib.Grids()
         g.flat, g.offs, g.dims, g.origin, g.lo, g.hi = [_lib.ptr(t) for t in self.t_grid]
         g.R, g.dtype, g.spacing, g.penalty = int(gs.origin.shape[0]), code, float(gs.spacing), float(gs.penalty)
+        g.nmaps = _lib.ptr(self.t_nmaps)
         self.c_grids = g
         # receptor atoms for exact mode
         r = _lib.Receptors()
@@ -138,11 +141,36 @@ class B200KernelProblem:
         self.mc_variant = tune_mc(self, self._i32(chain_lig), state.contiguous())
         return self.mc_variant
 
+    def prop_features(self, chain_lig, state):
+        """Proposal-network feature rows [N, 288] (BF16) of N states."""
+        N = state.shape[0]
+        out = torch.empty(N, 288, dtype=torch.bfloat16, device=self.device)
+        cl = self._i32(chain_lig)
+        st = state.to(self.device, torch.float32).contiguous()
+        with torch.cuda.device(self.device):
+            _lib.call("adock_prop_features", self.c_lig, self.c_work, self.c_grids, self.c_sf, _lib.ptr(cl), N,
+                      _lib.ptr(st), _lib.ptr(out), _lib.stream_ptr())
+        return out
+
+    def prop_sample(self, chain_lig, chain_id, net_out, k, seed, segment):
+        """Moves [N, k, 32] drawn from the network's Gaussian (net_out [N, 64])."""
+        N = net_out.shape[0]
+        moves = torch.empty(N, k, 32, device=self.device)
+        cl, ci = self._i32(chain_lig), self._i32(chain_id)
+        no = net_out.float().contiguous()
+        with torch.cuda.device(self.device):
+            _lib.call("adock_prop_sample", self.c_lig, self.c_work, _lib.ptr(cl), _lib.ptr(ci), N, _lib.ptr(no), int(k),
+                      int(seed) & 0xFFFFFFFFFFFFFFFF, int(segment), _lib.ptr(moves), _lib.stream_ptr())
+        return moves
+
     def run_mc(self, chain_lig, chain_id, cur, cur_e, best, best_e, init_opt, mc_steps, bfgs_iters, temp,
-               amp_pos, amp_rot, seed, step_offset, exact=False, nbr=None, nbr_n=None, order=None, variant=None):
+               amp_pos, amp_rot, seed, step_offset, exact=False, nbr=None, nbr_n=None, order=None, variant=None,
+               prop=None, prop_stats=None, log=None):
         """In place on cur/cur_e/best/best_e (float32 contiguous CUDA tensors). exact=True with nbr [N, NB] int32 /
         nbr_n [N]: each chain's exact inter energy loops only over its receptor-atom neighbour list.
-        variant: MC launch variant (default: the tuned one, else the library default)."""
+        variant: MC launch variant (default: the tuned one, else the library default).
+        prop: learned moves [N, k, 32] for steps 0..k-1 of this launch (plain MC fallback after 8 rejections);
+        prop_stats: int64 [4] counters; log: (x BF16 [cap, 288], y [cap, 32], n int32 [1]) training-data log."""
         N = cur.shape[0]
         if N == 0:
             return
@@ -170,6 +198,15 @@ class B200KernelProblem:
         a.step_offset, a.exact = int(step_offset), int(exact)
         a.order, a.queue, a.evals = _lib.ptr(order), _lib.ptr(self.queue), _lib.ptr(self.evals)
         a.variant = int(getattr(self, "mc_variant", 0) if variant is None else variant)
+        if prop is not None:
+            assert prop.is_contiguous() and prop.shape[0] == N and prop.shape[2] == 32 and prop.dtype == torch.float32
+            a.prop, a.prop_k = _lib.ptr(prop), int(prop.shape[1])
+            keep.append(prop)
+        if prop_stats is not None:
+            a.prop_stats = _lib.ptr(prop_stats)
+        if log is not None:
+            lx, ly, ln = log
+            a.log_x, a.log_y, a.log_n, a.log_cap = _lib.ptr(lx), _lib.ptr(ly), _lib.ptr(ln), int(lx.shape[0])
         with torch.cuda.device(self.device):
             _lib.call("adock_mc", self.c_lig, self.c_work, self.c_grids, self.c_sf, self.c_rec, a, _lib.stream_ptr())
         self._keep_mc = keep

@@ -1,0 +1,294 @@
+"""Learned Monte-Carlo proposal (no reference counterpart).
+
+A small MLP proposes the MC move of each chain: x [288 features of the chain's current state] -> SiLU(256) ->
+SiLU(256) -> 64 outputs = Gaussian means (columns 0..25) and log standard deviations (32..57) of the move
+(translation 3 A, rotation vector 3 rad, torsion deltas 20 rad). Weights are BF16 on the tensor cores with FP32
+accumulation; training keeps FP32 master weights and Adam moments. Every kernel is the library's own
+(adock_gemm_bf16, adock_mlp_nll, adock_silu_backward, adock_bias_grad, adock_adam).
+
+Training data are the plain search's own accepted improving moves (``collect``): the MC kernel logs, for each
+accepted move that lowered the chain's energy, the features of the pre-move state and the move to the accepted
+BFGS minimum. In the search (``run_mc_segments``) the network's moves replace the random perturbation; the
+Vina-form energy with BFGS and the Metropolis test still judge every move, and a chain whose learned moves are
+rejected 8 times in a row falls back to plain MC until it accepts a move.
+"""
+from __future__ import annotations
+
+import math
+
+import torch
+
+from . import _lib
+
+IN, HID, OUT = 288, 256, 64
+
+
+def _gemm(A, sA, B, sB, M, N, K, C=None, beta=0.0, bias=None, act=0, pre=None, Cb=None):
+    """C[M,N] = A[M,K] B[K,N] (BF16 operands with (row, col) strides sA, sB; FP32 accumulation)."""
+    _lib.call("adock_gemm_bf16", M, N, K, _lib.ptr(A), sA[0], sA[1], _lib.ptr(B), sB[0], sB[1], _lib.ptr(C),
+              N if C is not None else 0, float(beta), _lib.ptr(bias), int(act), _lib.ptr(pre), _lib.ptr(Cb),
+              N if Cb is not None else 0, _lib.stream_ptr())
+
+
+class ProposalNet:
+    """288 -> 256 -> 256 -> 64 MLP; weights W_i stored [K, N] row-major (x @ W)."""
+
+    def __init__(self, device="cuda", seed=0, init_log_sd=(0.0, -1.0, -0.5)):
+        dev = torch.device(device)
+        g = torch.Generator(device="cpu").manual_seed(seed)
+        dims = [(IN, HID), (HID, HID), (HID, OUT)]
+        self.W = [(torch.randn(k, n, generator=g) * math.sqrt(2.0 / k)).to(dev) for k, n in dims]
+        self.W[2].mul_(0.01)
+        self.b = [torch.zeros(n, device=dev) for _, n in dims]
+        # initial spread: log sd for translation, rotation, torsion columns
+        self.b[2][32:35] = init_log_sd[0]
+        self.b[2][35:38] = init_log_sd[1]
+        self.b[2][38:58] = init_log_sd[2]
+        self.params = self.W + self.b
+        self.Wb = [w.to(torch.bfloat16).contiguous() for w in self.W]
+        self.m = [torch.zeros_like(p) for p in self.params]
+        self.v = [torch.zeros_like(p) for p in self.params]
+        self.step = 0
+        self.device = dev
+
+    def state_dict(self):
+        return {"W": [w.cpu() for w in self.W], "b": [b.cpu() for b in self.b], "step": self.step}
+
+    def load_state_dict(self, d):
+        for dst, src in zip(self.W + self.b, d["W"] + d["b"]):
+            dst.copy_(src.to(self.device))
+        self.Wb = [w.to(torch.bfloat16).contiguous() for w in self.W]
+        self.step = int(d.get("step", 0))
+
+    def forward(self, x, save=False):
+        """x: BF16 [B, 288] -> out FP32 [B, 64] (and saved activations when save)."""
+        B = x.shape[0]
+        dev = self.device
+        pre1 = torch.empty(B, HID, device=dev)
+        h1 = torch.empty(B, HID, dtype=torch.bfloat16, device=dev)
+        pre2 = torch.empty(B, HID, device=dev)
+        h2 = torch.empty(B, HID, dtype=torch.bfloat16, device=dev)
+        out = torch.empty(B, OUT, device=dev)
+        c1 = torch.empty(B, HID, device=dev)
+        c2 = torch.empty(B, HID, device=dev)
+        with torch.cuda.device(dev):
+            _gemm(x, (IN, 1), self.Wb[0], (HID, 1), B, HID, IN, C=c1, bias=self.b[0], act=1, pre=pre1, Cb=h1)
+            _gemm(h1, (HID, 1), self.Wb[1], (HID, 1), B, HID, HID, C=c2, bias=self.b[1], act=1, pre=pre2, Cb=h2)
+            _gemm(h2, (HID, 1), self.Wb[2], (OUT, 1), B, OUT, HID, C=out, bias=self.b[2])
+        if save:
+            return out, (x, pre1, h1, pre2, h2)
+        return out
+
+    def loss_grad(self, x, y):
+        """Mean Gaussian NLL of moves y [B, 32] and the parameter gradients (list matching self.params)."""
+        B = x.shape[0]
+        dev = self.device
+        out, (x, pre1, h1, pre2, h2) = self.forward(x, save=True)
+        dout = torch.empty(B, OUT, dtype=torch.bfloat16, device=dev)
+        loss = torch.zeros(1, device=dev)
+        gW = [torch.empty_like(w) for w in self.W]
+        gb = [torch.empty_like(b) for b in self.b]
+        dH2 = torch.empty(B, HID, device=dev)
+        dA2 = torch.empty(B, HID, dtype=torch.bfloat16, device=dev)
+        dH1 = torch.empty(B, HID, device=dev)
+        dA1 = torch.empty(B, HID, dtype=torch.bfloat16, device=dev)
+        s = _lib.stream_ptr
+        with torch.cuda.device(dev):
+            _lib.call("adock_mlp_nll", _lib.ptr(out), _lib.ptr(y), B, _lib.ptr(dout), _lib.ptr(loss), s())
+            # layer 3: dW3 = h2^T dout, db3, dH2 = dout W3^T
+            _gemm(h2, (1, HID), dout, (OUT, 1), HID, OUT, B, C=gW[2])
+            _lib.call("adock_bias_grad", _lib.ptr(dout), B, OUT, _lib.ptr(gb[2]), s())
+            _gemm(dout, (OUT, 1), self.Wb[2], (1, OUT), B, HID, OUT, C=dH2)
+            _lib.call("adock_silu_backward", _lib.ptr(dH2), _lib.ptr(pre2), B * HID, _lib.ptr(dA2), s())
+            # layer 2
+            _gemm(h1, (1, HID), dA2, (HID, 1), HID, HID, B, C=gW[1])
+            _lib.call("adock_bias_grad", _lib.ptr(dA2), B, HID, _lib.ptr(gb[1]), s())
+            _gemm(dA2, (HID, 1), self.Wb[1], (1, HID), B, HID, HID, C=dH1)
+            _lib.call("adock_silu_backward", _lib.ptr(dH1), _lib.ptr(pre1), B * HID, _lib.ptr(dA1), s())
+            # layer 1
+            _gemm(x, (1, IN), dA1, (HID, 1), IN, HID, B, C=gW[0])
+            _lib.call("adock_bias_grad", _lib.ptr(dA1), B, HID, _lib.ptr(gb[0]), s())
+        return loss / B, gW + gb
+
+    def train_step(self, x, y, lr=1e-3, wd=0.0):
+        loss, grads = self.loss_grad(x, y)
+        self.step += 1
+        with torch.cuda.device(self.device):
+            for i, (p, g_, m, v) in enumerate(zip(self.params, grads, self.m, self.v)):
+                pb = self.Wb[i] if i < 3 else None
+                _lib.call("adock_adam", _lib.ptr(p), _lib.ptr(g_), _lib.ptr(m), _lib.ptr(v), _lib.ptr(pb), p.numel(),
+                          float(lr), 0.9, 0.999, 1e-8, self.step, float(wd), _lib.stream_ptr())
+        return loss
+
+    def fit(self, X, Y, epochs=3, batch=4096, lr=1e-3, seed=0, log=None):
+        """Minibatch Adam over (X BF16 [n, 288], Y [n, 32]); returns the mean loss of the last epoch."""
+        n = X.shape[0]
+        g = torch.Generator(device=self.device).manual_seed(seed)
+        last = float("nan")
+        for ep in range(epochs):
+            perm = torch.randperm(n, generator=g, device=self.device)
+            tot = torch.zeros(1, device=self.device)
+            nb = 0
+            for i in range(0, n - batch + 1, batch):
+                idx = perm[i:i + batch]
+                tot += self.train_step(X[idx].contiguous(), Y[idx].contiguous(), lr=lr)
+                nb += 1
+            last = float(tot) / max(nb, 1)
+            if log is not None:
+                log(f"epoch {ep}: loss {last:.4f}")
+        return last
+
+
+def collect(kp, chain_lig, chain_id, cur, cur_e, best, best_e, cfg, seed, cap, init_opt=True):
+    """Run the plain MC search on the given chains with the training-data log on; returns (X BF16 [n, 288],
+    Y [n, 32]) of accepted improving moves (n <= cap)."""
+    dev = kp.device
+    lx = torch.empty(cap, IN, dtype=torch.bfloat16, device=dev)
+    ly = torch.empty(cap, 32, device=dev)
+    ln = torch.zeros(1, dtype=torch.int32, device=dev)
+    kp.run_mc(chain_lig, chain_id, cur, cur_e, best, best_e, init_opt, cfg["mc_steps"], cfg["bfgs_iters"],
+              cfg["mc_temperature"], cfg["mc_amp_pos"], cfg["mc_amp_rot"], seed, 0, log=(lx, ly, ln))
+    n = min(int(ln), cap)
+    return lx[:n], ly[:n]
+
+
+def _starts(prob, kp, cfg, seed):
+    """Stage-A start poses of every chain (the search driver's first stage), packed as MC states."""
+    from .search import stage_a_kernel
+    dev = kp.device
+    L, M = prob.lb.L, cfg["n_chains"]
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    bc = ((prob.gs.lo[0] + prob.gs.hi[0]) / 2)[None].expand(L, 3)
+    bs = [(prob.gs.hi[0] - prob.gs.lo[0]).cpu().numpy()] * L
+    t, q0, th, _ = stage_a_kernel(prob, kp, bc, bs, cfg, gen)
+    N = L * M
+    cur = kp.pack(t.reshape(N, 3), q0.reshape(N, 4), th.reshape(N, -1))
+    chain_lig = torch.arange(L, device=dev, dtype=torch.int32).repeat_interleave(M)
+    chain_id = torch.arange(N, device=dev, dtype=torch.int32)
+    return chain_lig, chain_id, cur
+
+
+def _problem_for(rec, ligs, dev, grid_dtype="f32"):
+    import numpy as np
+    from . import params
+    from .grid import make_gridset
+    from .kernel import B200KernelProblem
+    from .ligand import LigandBatch
+    from .problem import PairPotential, Problem, pad_receptors
+    sfp = params.sf_params("vina")
+    types = np.unique(np.concatenate([l.types for l in ligs]))
+    gs = make_gridset([rec], sfp, params.GRID_SPACING, params.OUT_OF_BOX_PENALTY, device=dev, lig_types=[types])
+    prob = Problem(gs, LigandBatch(ligs, dev), torch.zeros(len(ligs), dtype=torch.long, device=dev),
+                   PairPotential(sfp, dev), rec=pad_receptors([rec], dev))
+    return prob, B200KernelProblem(prob, grid_dtype=grid_dtype)
+
+
+def _best_per_ligand(best_e, L, M):
+    return best_e.view(L, M).min(1).values
+
+
+def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(250, 500, 1000, 2000),
+               ref_steps=8000, train_steps=500, log_cap=2_000_000, epochs=3, prop_k=8, seed=0, log=None):
+    """Learned proposal vs plain MC at equal step budget (config-3 style evaluation).
+
+    1. Training data: plain FP32 search (Stage-A starts, ``train_steps`` MC steps) on ``train_ligs`` with the
+       move log on; the network is trained on it (``epochs`` of Adam).
+    2. Reference: plain FP32 search with ``ref_steps`` steps on the held-out ``eval_ligs``; E_ref(l) = the lowest
+       best energy over the ligand's chains (also over all runs below, so gaps are >= 0).
+    3. For each budget S: plain FP32, plain FP16 and learned FP16 (proposals, plain fallback) from the same
+       Stage-A starts; gap(l) = E(l) - E_ref(l); reported: median gap and ligands/s of Stage A + MC.
+    """
+    dev = torch.device(device)
+    from . import params
+    cfg_tr = params.workload_preset(chains, train_steps)
+    out = {"chains": chains, "budgets": list(budgets), "ref_steps": ref_steps, "train_ligands": len(train_ligs),
+           "eval_ligands": len(eval_ligs)}
+    # 1. data + training
+    prob_t, kp_t = _problem_for(rec, train_ligs, dev)
+    cl, ci, cur = _starts(prob_t, kp_t, cfg_tr, seed)
+    N = cur.shape[0]
+    best = cur.clone()
+    ce, be = torch.zeros(N, device=dev), torch.full((N,), float("inf"), device=dev)
+    torch.cuda.synchronize(dev)
+    X, Y = collect(kp_t, cl, ci, cur, ce, best, be, cfg_tr, seed=seed + 1, cap=log_cap)
+    net = ProposalNet(dev, seed=seed)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    loss = net.fit(X, Y, epochs=epochs, batch=4096, lr=1e-3, seed=seed, log=log)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    out["train"] = {"moves": int(X.shape[0]), "epochs": epochs, "final_loss": loss, "train_ms": e0.elapsed_time(e1),
+                    "loss_untrained": float(ProposalNet(dev, seed=seed).loss_grad(X[:65536], Y[:65536])[0])}
+    del X, Y, kp_t, prob_t
+    # 2./3. evaluation on held-out ligands
+    probs = {"f32": _problem_for(rec, eval_ligs, dev, "f32")}
+    probs["f16"] = (probs["f32"][0], type(probs["f32"][1])(probs["f32"][0], grid_dtype="f16"))
+    L = len(eval_ligs)
+
+    def run(method, steps):
+        prob, kp = probs["f16" if method != "plain_f32" else "f32"]
+        cfg = params.workload_preset(chains, steps)
+        cfg["autotune"] = False
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record()
+        cl, ci, cur = _starts(prob, kp, cfg, seed + 2)
+        best = cur.clone()
+        ce, be = torch.zeros(cur.shape[0], device=dev), torch.full((cur.shape[0],), float("inf"), device=dev)
+        st = {}
+        if method == "learned_f16":
+            run_mc_segments(kp, net, cl, ci, cur, ce, best, be, cfg, seed + 3, prop_k=prop_k, stats=st)
+        else:
+            kp.run_mc(cl, ci, cur, ce, best, be, True, steps, cfg["bfgs_iters"], cfg["mc_temperature"],
+                      cfg["mc_amp_pos"], cfg["mc_amp_rot"], seed + 3, 0)
+        ev[1].record()
+        torch.cuda.synchronize(dev)
+        return _best_per_ligand(be, L, chains), ev[0].elapsed_time(ev[1]), st
+
+    ref, ref_ms, _ = run("plain_f32", ref_steps)
+    results = {}
+    for m in ("plain_f32", "plain_f16", "learned_f16"):
+        for S in budgets:
+            results[(m, S)] = run(m, S)
+    floor = ref.clone()
+    for (e, _, _) in results.values():
+        floor = torch.minimum(floor, e)
+    out["reference"] = {"ms": ref_ms, "median_best": float(ref.median())}
+    rows = {}
+    for (m, S), (e, ms, st) in results.items():
+        gap = (e - floor).cpu()
+        rows.setdefault(m, []).append({"steps": S, "median_gap": float(gap.median()), "mean_gap": float(gap.mean()),
+                                       "ligands_per_s": L / (ms / 1e3), "ms": ms, **st})
+    out["methods"] = rows
+    # equal-gap comparison: the budget each method needs to reach the plain FP32 median gap at its largest budget
+    target = rows["plain_f32"][-1]["median_gap"]
+    out["target_gap"] = target
+    for m, rs in rows.items():
+        ok = [r for r in rs if r["median_gap"] <= target + 1e-6]
+        out.setdefault("at_target_gap", {})[m] = ({"steps": ok[0]["steps"], "ligands_per_s": ok[0]["ligands_per_s"]}
+                                                  if ok else None)
+    a = out["at_target_gap"]
+    if a.get("learned_f16") and a.get("plain_f32"):
+        out["speedup_at_equal_gap"] = a["learned_f16"]["ligands_per_s"] / a["plain_f32"]["ligands_per_s"]
+    return out
+
+
+def run_mc_segments(kp, net, chain_lig, chain_id, cur, cur_e, best, best_e, cfg, seed, prop_k=8, init_opt=True,
+                    stats=None):
+    """MC with learned proposals: the run is cut into segments of prop_k steps; before each segment the network
+    reads every chain's current state and draws prop_k moves per chain (adock_prop_sample); the MC kernel applies
+    them in order (plain MC after 8 consecutive rejections)."""
+    steps = cfg["mc_steps"]
+    pst = torch.zeros(4, dtype=torch.int64, device=kp.device)
+    for sg in range(math.ceil(steps / prop_k)):
+        k = min(prop_k, steps - sg * prop_k)
+        feat = kp.prop_features(chain_lig, cur)
+        out = net.forward(feat)
+        moves = kp.prop_sample(chain_lig, chain_id, out, k, seed ^ 0x5EEDBA5E, sg)
+        kp.run_mc(chain_lig, chain_id, cur, cur_e, best, best_e, init_opt and sg == 0, k, cfg["bfgs_iters"],
+                  cfg["mc_temperature"], cfg["mc_amp_pos"], cfg["mc_amp_rot"], seed, sg * prop_k, prop=moves,
+                  prop_stats=pst)
+    if stats is not None:
+        p, pa, q, qa = pst.tolist()
+        stats.update(prop_steps=p, prop_accepted=pa, plain_steps=q, plain_accepted=qa)
+    return pst

@@ -46,6 +46,9 @@ def _args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the map-builder / map-precision section")
+    ap.add_argument("--ab", action="store_true", help="learned proposal vs plain MC at equal step budget")
+    ap.add_argument("--ab-train", type=int, default=256, help="fresh ligands for the proposal's training data")
+    ap.add_argument("--ab-eval", type=int, default=256, help="held-out ligands for the A/B comparison")
     return ap.parse_args()
 
 
@@ -310,6 +313,12 @@ def run_ours(args, rank, world, local_rank):
            "mc_autotune": __import__("adock_b200.autotune", fromlist=["cached"]).cached()}
     if rank == 0 and world == 1 and not args.no_extras:
         out["grid_and_precision"] = _grid_and_precision(dev, ligs)
+    if rank == 0 and world == 1 and args.ab:
+        from adock_b200 import synth
+        from adock_b200.proposal import ab_compare
+        train = synth.ligand_set(args.ab_train, (10, 60), (0, 15), seed0=100_000)
+        held = synth.ligand_set(args.ab_eval, (10, 60), (0, 15), seed0=200_000)
+        out["learned_proposal"] = ab_compare(rec, train, held, device=dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = _cpu_baseline(ligs, rec, cfg)
     return out

@@ -75,6 +75,7 @@ typedef struct {
     int R;
     int dtype;                 /* ADOCK_GRID_* of flat */
     float spacing, penalty;
+    const int* nmaps;          /* [R] maps per receptor (dev, may be NULL: 8 assumed by the proposal features) */
 } adock_grids_t;
 
 /* Receptor atoms for the exact (grid-free) energy, dev; xyz == NULL when absent. */
@@ -114,6 +115,17 @@ typedef struct {
     int* queue;                /* dev, 1 int work counter, zeroed by the call on `stream` */
     unsigned long long* evals; /* dev, 2 counters (accumulated): energy evaluations, atom evaluations; or NULL */
     int variant;               /* launch variant (0 = default; 1-3 = 4, 6, 8 resident blocks per SM), autotuned */
+    /* learned proposal (no reference counterpart): moves [N, prop_k, 32] for the launch's steps (NULL = plain MC);
+     * after 8 consecutive rejections of proposed moves a chain falls back to plain MC until a move is accepted */
+    const float* prop;
+    int prop_k;
+    unsigned long long* prop_stats; /* dev [4] or NULL: proposed, proposed+accepted, plain, plain+accepted */
+    /* training-data log (NULL = off): each accepted improving move appends features [288] (BF16) of the pre-move
+     * state and the move [32] (translation 3, rotation vector 3, torsions 20, torsion count) while *log_n < cap */
+    void* log_x;
+    float* log_y;
+    int* log_n;
+    int log_cap;
 } adock_mc_args_t;
 
 /* ------------------------------------------------------------------------------------------------ misc */
@@ -181,6 +193,36 @@ int adock_neighbours(const adock_ligands_t* lig, const adock_work_t* work, const
 int adock_rescore64(const adock_ligands_t* lig, const adock_work_t* work, const adock_grids_t* grids,
                     const adock_sf_t* sf, const adock_receptors_t* rec, const int* chain_lig, int n,
                     const float* state, double* e_total, double* e_intra, float* X, void* stream);
+
+/* ------------------------------------------------------------------------------------------------ proposal net */
+/* No reference counterpart: the learned MC proposal. Network 288 -> 256 (SiLU) -> 256 (SiLU) -> 64, BF16
+ * weights, FP32 accumulation; output columns 0..25 = move means, 32..57 = log standard deviations. */
+
+/* Feature rows (BF16 [n, 288], dev) of n states (layout in csrc/search_impl.cuh prop_features). */
+int adock_prop_features(const adock_ligands_t* lig, const adock_work_t* work, const adock_grids_t* grids,
+                        const adock_sf_t* sf, const int* chain_lig, int n, const float* state, void* feat,
+                        void* stream);
+/* Moves [n, k, 32] (dev) drawn from the network output [n, 64]: move = mean + exp(log_sd) * z, z standard normal
+ * from a counter-based stream of (seed, chain_id, segment, slot); torsion entries past a ligand's count are 0. */
+int adock_prop_sample(const adock_ligands_t* lig, const adock_work_t* work, const int* chain_lig, const int* chain_id,
+                      int n, const float* net_out, int k, unsigned long long seed, int segment, float* moves,
+                      void* stream);
+/* C[M,N] = A[M,K] B[K,N] on the tensor cores (BF16 operands at any strides, FP32 accumulation); epilogue
+ * C = acc + beta C + bias, optional pre-activation copy, optional SiLU (act = 1), optional BF16 copy Cb. */
+int adock_gemm_bf16(int M, int N, int K, const void* A, long long sAm, long long sAk, const void* B, long long sBk,
+                    long long sBn, float* C, long long ldc, float beta, const float* bias, int act, float* pre,
+                    void* Cb, long long ldcb, void* stream);
+/* Gaussian NLL of moves target [B, 32] under out [B, 64]; dout (BF16 [B, 64]) = gradient of the batch mean;
+ * *loss += summed NLL. */
+int adock_mlp_nll(const float* out, const float* target, int B, void* dout, float* loss, void* stream);
+/* dA = dH * SiLU'(A), BF16 output. */
+int adock_silu_backward(const float* dH, const float* A, long long n, void* dA, void* stream);
+/* db = column sums of dA (BF16 [rows, cols]). */
+int adock_bias_grad(const void* dA, int rows, int cols, float* db, void* stream);
+/* Adam step on FP32 master parameters p (with BF16 copy pb, may be NULL). */
+int adock_adam(float* p, const float* grad, float* m, float* v, void* pb, long long n, float lr, float b1, float b2,
+               float eps, int step, float wd, void* stream);
+int adock_f32_to_bf16(const float* x, void* y, long long n, void* stream);
 
 /* ------------------------------------------------------------------------------------------------ no allocation */
 

@@ -1,0 +1,127 @@
+"""Learned proposal on the B200: tensor-core GEMM against torch, network gradients against the float64 oracle
+(oracle/mlp.py), feature rows and the training-data log of the MC kernel, training, and the proposal-driven MC
+with its plain-MC fallback."""
+import numpy as np
+import pytest
+import torch
+
+from helpers import ligands, lig_types, make_problem, oracle_grid, receptor, random_states
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def dev():
+    assert torch.cuda.is_available()
+    return torch.device("cuda:0")
+
+
+@pytest.mark.parametrize("M,N,K,ta,tb", [(64, 64, 32, 0, 0), (100, 72, 40, 0, 0), (257, 256, 288, 1, 0),
+                                         (256, 64, 1000, 1, 0), (333, 256, 64, 0, 1), (1, 7, 5, 1, 1)])
+def test_gemm_bf16_matches_torch(dev, M, N, K, ta, tb):
+    from adock_b200.proposal import _gemm
+    g = torch.Generator(device=dev).manual_seed(M * 7 + N)
+    A = torch.randn(K, M, device=dev, generator=g).to(torch.bfloat16) if ta else \
+        torch.randn(M, K, device=dev, generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, device=dev, generator=g).to(torch.bfloat16) if tb else \
+        torch.randn(K, N, device=dev, generator=g).to(torch.bfloat16)
+    Am = A.t() if ta else A
+    Bm = B.t() if tb else B
+    sA = (1, M) if ta else (K, 1)
+    sB = (1, K) if tb else (N, 1)
+    C = torch.empty(M, N, device=dev)
+    bias = torch.randn(N, device=dev, generator=g)
+    with torch.cuda.device(dev):
+        _gemm(A, sA, B, sB, M, N, K, C=C, bias=bias)
+    ref = Am.float() @ Bm.float() + bias
+    torch.testing.assert_close(C, ref, rtol=1e-4, atol=1e-3)
+
+
+def test_network_gradients_match_float64_oracle(dev):
+    from oracle import mlp as O
+    from adock_b200.proposal import ProposalNet
+    net = ProposalNet(dev, seed=3)
+    for w in net.W:   # a non-trivial network
+        w.add_(torch.randn_like(w) * 0.05)
+    net.Wb = [w.to(torch.bfloat16).contiguous() for w in net.W]
+    g = torch.Generator(device=dev).manual_seed(1)
+    B = 512
+    X = torch.randn(B, 288, device=dev, generator=g).to(torch.bfloat16)
+    Y = torch.randn(B, 32, device=dev, generator=g) * 0.5
+    Y[:, 26] = torch.randint(0, 21, (B,), device=dev, generator=g).float()
+    Y[:, 27:] = 0
+    loss, grads = net.loss_grad(X, Y)
+    Wr = [w.to(torch.bfloat16).double().cpu().numpy() for w in net.W]
+    lo, go = O.loss_and_grads(Wr, [b.double().cpu().numpy() for b in net.b], X.double().cpu().numpy(),
+                              Y.double().cpu().numpy())
+    assert abs(float(loss) - lo) <= 1e-2 * max(1.0, abs(lo))
+    for gg, gr in zip(grads, go):
+        gg = gg.double().cpu().numpy()
+        assert np.linalg.norm(gg - gr) <= 2e-2 * np.linalg.norm(gr) + 1e-6
+
+
+def _problem(dev):
+    from adock_b200 import params
+    sfp = params.sf_params("vina")
+    rec = receptor("cfg0")
+    ligs = ligands("mixed")
+    lt = lig_types(ligs)
+    G = oracle_grid(rec, sfp, lt) if _have_ref() else None
+    if G is None:
+        from adock_b200.grid import build_grid, grid_dims
+        o = rec["center"] - rec["size"] / 2
+        G = build_grid(rec["rec_xyz"], rec["rec_types"], sfp, o, params.GRID_SPACING,
+                       grid_dims(rec["size"], params.GRID_SPACING), lt, device=dev).cpu().numpy()
+    return make_problem(rec, ligs, sfp, G, lt, dev)
+
+
+def _have_ref():
+    from oracle import ref
+    return ref.available()
+
+
+def test_features_log_training_and_proposal_mc(dev):
+    from adock_b200 import params
+    from adock_b200.kernel import B200KernelProblem
+    from adock_b200.proposal import ProposalNet, collect, run_mc_segments
+    prob = _problem(dev)
+    kp = B200KernelProblem(prob)
+    cl, st = random_states(prob, 32, seed=7, sigma=1.0)
+    cl = torch.as_tensor(cl, device=dev)
+    st = torch.as_tensor(st, device=dev)
+    M = len(cl)
+    ci = torch.arange(M, dtype=torch.int32, device=dev)
+    # feature rows: finite, torsion sin/cos zero beyond each ligand's count, descriptors as documented
+    F = kp.prop_features(cl, st).float().cpu().numpy()
+    assert F.shape == (M, 288) and np.isfinite(F).all()
+    for i in range(M):
+        p = prob.lb.preps[int(cl[i])]
+        assert abs(F[i, 263] - p.n / 64) < 1e-2 and abs(F[i, 264] - p.n_tors / 20) < 1e-2
+        assert np.all(F[i, 223 + 2 * p.n_tors:263] == 0) and np.all(F[i, 275:] == 0)
+        assert abs(np.linalg.norm(F[i, 219:223]) - 1) < 2e-2 and F[i, 219] >= 0
+    # training-data log of the plain search
+    cfg = params.workload_preset(32, 6)
+    cur, best = st.clone(), st.clone()
+    ce, be = torch.zeros(M, device=dev), torch.full((M,), float("inf"), device=dev)
+    X, Y = collect(kp, cl, ci, cur, ce, best, be, cfg, seed=5, cap=100000)
+    assert X.shape[0] > M  # several improving moves per chain
+    Yn = Y.cpu().numpy()
+    assert np.isfinite(Yn).all() and np.all(np.abs(Yn[:, 6:26]) <= np.pi + 1e-4)
+    nt = Yn[:, 26].astype(int)
+    for i in range(len(Yn)):
+        assert np.all(Yn[i, 6 + nt[i]:26] == 0)
+    # training lowers the loss
+    net = ProposalNet(dev, seed=0)
+    l0 = float(net.loss_grad(X, Y)[0])
+    net.fit(X, Y, epochs=30, batch=min(256, X.shape[0]), lr=3e-3)
+    l1 = float(net.loss_grad(X, Y)[0])
+    assert l1 < l0
+    # proposal-driven MC: energies are consistent and the fallback accounting adds up
+    cur, best = st.clone(), st.clone()
+    ce, be = torch.zeros(M, device=dev), torch.full((M,), float("inf"), device=dev)
+    stats = {}
+    run_mc_segments(kp, net, cl, ci, cur, ce, best, be, cfg, seed=9, prop_k=4, stats=stats)
+    e_best, _ = kp.energy_grad(cl, best)
+    torch.testing.assert_close(e_best, be, rtol=1e-4, atol=1e-4)
+    assert stats["prop_steps"] + stats["plain_steps"] == M * cfg["mc_steps"]
+    assert stats["prop_steps"] > 0
