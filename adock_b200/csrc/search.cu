@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(256) neighbours_kernel(const __grid_constant__
 }
 
 // ------------------------------------------------------------------------------------------ proposal sampling
-// moves[c, k, d] = mean[c, d] + exp(clamp(log_sd[c, d], -4, 2)) * z, z ~ N(0, 1) by Box-Muller on the counter-based
+// moves[c, k, d] = mean[c, d] + max(exp(clamp(log_sd[c, d], -4, 2)), floor_d) * z, z ~ N(0, 1) by Box-Muller on the counter-based
 // stream (seed, chain id, 64 * segment + k, 2 d / 2 d + 1); torsion entries past the ligand's count are 0.
 __global__ void prop_sample_kernel(const int4* info, const int* chain_lig, const int* chain_id, int n,
                                    const float* out, int k, unsigned long long seed, int segment, float* moves) {
@@ -210,7 +210,9 @@ __global__ void prop_sample_kernel(const int4* info, const int* chain_lig, const
         const float z = sqrtf(-2.f * __logf(u1)) * __cosf(6.28318531f * u2);
         const float mu = out[(long long)c * 64 + d];
         const float ls = fminf(fmaxf(out[(long long)c * 64 + 32 + d], -4.f), 2.f);
-        v = mu + __expf(ls) * z;
+        // floors on the spread (0.5 A, 0.25 rad, 0.5 rad) keep the sampled moves exploring
+        const float floor_sd = d < 3 ? 0.5f : (d < 6 ? 0.25f : 0.5f);
+        v = mu + fmaxf(__expf(ls), floor_sd) * z;
     }
     moves[idx] = v;
 }
@@ -327,6 +329,7 @@ extern "C" int adock_mc(const adock_ligands_t* lig, const adock_work_t* work, co
     ADOCK_CHECK_ARG(!mc->prop || mc->prop_k >= 1, "prop_k must be >= 1 with proposals");
     ADOCK_CHECK_ARG(!mc->log_x || (mc->log_y && mc->log_n && mc->log_cap >= 0), "incomplete training-data log");
     M.prop = mc->prop; M.prop_k = mc->prop_k; M.prop_stats = mc->prop_stats;
+    M.prop_frac = (mc->prop_frac <= 0.f || mc->prop_frac >= 1.f) ? 1.f : mc->prop_frac;
     M.log_x = (__nv_bfloat16*)mc->log_x; M.log_y = mc->log_y; M.log_n = mc->log_n; M.log_cap = mc->log_cap;
     const TypeTables tt = make_tables(sf);
     cudaStream_t st = (cudaStream_t)stream;

@@ -12,6 +12,18 @@
 namespace adock {
 
 #define EPSF 1.1920929e-07f
+
+// Code-size knobs of the MC kernel (instruction-cache footprint vs register allocation across calls).
+#ifdef ADOCK_BFGS_INLINE
+#define ADOCK_BFGS_ATTR __forceinline__
+#else
+#define ADOCK_BFGS_ATTR __noinline__
+#endif
+#ifdef ADOCK_COLD_NOINLINE
+#define ADOCK_COLD_ATTR __noinline__
+#else
+#define ADOCK_COLD_ATTR __forceinline__
+#endif
 #define PAIR_ROUNDS_MAX 256   // pair schedule: at most 256 rounds of 32 (8,192 pairs) are reordered
 
 struct SearchParams {
@@ -69,6 +81,7 @@ struct McParams {
     // learned proposal: moves [N, prop_k, 32] for steps 0..prop_k-1 of this launch (NULL: plain MC only)
     const float* prop;
     int prop_k;
+    float prop_frac;                 // fraction of steps that take the learned move (the rest: plain MC)
     unsigned long long* prop_stats;  // [4] proposals made, proposals accepted, plain steps, plain accepted
     // training-data log of accepted improving moves: features [cap, 288] BF16, moves [cap, 32]
     __nv_bfloat16* log_x;
@@ -468,7 +481,7 @@ __device__ __forceinline__ void neg_hv(const float* H, const float* v, float* ou
 // inlined eval_eg, keeps the kernel small enough for the instruction cache (instruction-fetch stalls were the
 // largest stall reason with four inlined copies of eval_eg).
 template <int APL, typename GT>
-__device__ __noinline__ float bfgs(float* ws, const WSLayout& L, float* x, int iters, const Chain<APL>& c_in,
+__device__ ADOCK_BFGS_ATTR float bfgs(float* ws, const WSLayout& L, float* x, int iters, const Chain<APL>& c_in,
                                    const SearchParams& P, const TypeTables& tt, int lane, unsigned& n_eval) {
     const Chain<APL> c = c_in;   // registers for the whole optimisation
     const int D = 6 + c.nt, S = 7 + c.nt;
@@ -571,7 +584,8 @@ __device__ __noinline__ float bfgs(float* ws, const WSLayout& L, float* x, int i
 //              per map slot 0..7
 //   [275, 288) 0
 template <typename GT>
-__device__ void prop_features(const SearchParams& P, int l, const float* s, __nv_bfloat16* out, int lane) {
+__device__ ADOCK_COLD_ATTR void prop_features(const SearchParams& P, int l, const float* s, __nv_bfloat16* out,
+                                              int lane) {
     const int4 inf = P.info[l];
     const int na = inf.x, nt = inf.y, np = inf.z, ri = inf.w;
     const int nx = (int)P.dims[3 * ri], ny = (int)P.dims[3 * ri + 1], nz = (int)P.dims[3 * ri + 2];
@@ -616,33 +630,15 @@ __device__ void prop_features(const SearchParams& P, int l, const float* s, __nv
     __syncwarp();
 }
 
-// Move from state a to state b (proposal coordinates): translation, rotation vector of q_b q_a^-1, torsion
-// differences wrapped to [-pi, pi); entry 26 holds the torsion count. Lane 0 writes.
-__device__ __forceinline__ void state_move(const float* a, const float* b, int nt, float* y) {
-    y[0] = b[0] - a[0]; y[1] = b[1] - a[1]; y[2] = b[2] - a[2];
-    // r = q_b * conj(q_a)
-    const float aw = a[3], ax = -a[4], ay = -a[5], az = -a[6];
-    const float bw = b[3], bx = b[4], by = b[5], bz = b[6];
-    float w = bw * aw - bx * ax - by * ay - bz * az;
-    float x = bw * ax + bx * aw + by * az - bz * ay;
-    float yv = bw * ay - bx * az + by * aw + bz * ax;
-    float z = bw * az + bx * ay - by * ax + bz * aw;
-    const float nn = rsqrtf(w * w + x * x + yv * yv + z * z) * (w < 0.f ? -1.f : 1.f);
-    w *= nn; x *= nn; yv *= nn; z *= nn;
-    const float sn = sqrtf(x * x + yv * yv + z * z);
-    const float ang = 2.f * atan2f(sn, w);
-    const float k = sn > 1e-7f ? ang / sn : 2.f;
-    y[3] = x * k; y[4] = yv * k; y[5] = z * k;
-    for (int t = 0; t < 20; ++t) {
-        float d = 0.f;
-        if (t < nt) {
-            d = b[7 + t] - a[7 + t];
-            d = d - 6.28318531f * floorf((d + 3.14159265f) / 6.28318531f);
-        }
-        y[6 + t] = d;
-    }
-    y[26] = (float)nt;
-    for (int t = 27; t < 32; ++t) y[t] = 0.f;
+// Training-log row of a state (lane 0 writes): t (3), q (4), theta 0..19 (0 past the torsion count), torsion
+// count at 27, chain index at 28; the training target (the move to a later state of the same chain) is computed
+// after the run.
+static __device__ ADOCK_COLD_ATTR void log_state(const float* s, int nt, int ch, float* y) {
+    for (int i = 0; i < 7; ++i) y[i] = s[i];
+    for (int t = 0; t < 20; ++t) y[7 + t] = t < nt ? s[7 + t] : 0.f;
+    y[27] = (float)nt;
+    y[28] = (float)ch;
+    for (int t = 29; t < 32; ++t) y[t] = 0.f;
 }
 
 template <int APL, typename GT, int MINB>
@@ -696,7 +692,8 @@ __global__ void __launch_bounds__(128, MINB) mc_kernel(const __grid_constant__ S
             const int sg = M.step_offset + st;
             wcopy(x, cur, S, lane);
             // learned move while the proposal has not failed PROP_FAIL_MAX times in a row, else plain MC
-            const bool use_prop = M.prop && prop_fail < PROP_FAIL_MAX;
+            const bool use_prop = M.prop && prop_fail < PROP_FAIL_MAX &&
+                                  (M.prop_frac >= 1.f || uniform01(M.seed, cid, sg, 3) < M.prop_frac);
             if (use_prop) {
                 const float* mv = M.prop + ((long long)ch * M.prop_k + (st % M.prop_k)) * PROP_MOVE;
                 if (lane == 0) {
@@ -732,7 +729,7 @@ __global__ void __launch_bounds__(128, MINB) mc_kernel(const __grid_constant__ S
                 row = __shfl_sync(0xffffffffu, row, 0);
                 if (row < M.log_cap) {
                     prop_features<GT>(P, l, cur, M.log_x + (long long)row * PROP_IN, lane);
-                    if (lane == 0) state_move(cur, x, c.nt, M.log_y + (long long)row * PROP_MOVE);
+                    if (lane == 0) log_state(cur, c.nt, ch, M.log_y + (long long)row * PROP_MOVE);
                 }
                 __syncwarp();
             }

@@ -38,10 +38,15 @@ def dock_screen(receptor, box, ligands, cfg=None, device="cuda", seed=0, batch=N
     rec_t = pad_receptors([rec], dev)
     h2d = rec["rec_xyz"].nbytes + rec["rec_types"].nbytes + _nbytes(rec_t)
     B = len(ligands) if not batch else int(batch)
-    out = []
+    out = [None] * len(ligands)
     st_all = {}
-    for b0 in range(0, len(ligands), B):
-        chunk = list(ligands[b0:b0 + B])
+    # shape buckets: ligands with <= 64 heavy atoms and with more run in separate launches (the kernel's atoms per
+    # lane follow the largest ligand of a launch), each bucket in batches of B
+    nh = np.array([int(np.asarray(p.heavy).sum()) for p in ligands])
+    buckets = [np.where(nh <= 64)[0], np.where(nh > 64)[0]]
+    chunks = [idx[b0:b0 + B] for idx in buckets for b0 in range(0, len(idx), B)]
+    for idx in chunks:
+        chunk = [ligands[i] for i in idx]
         lb = LigandBatch(chunk, dev)
         h2d += _nbytes([lb.ref, lb.types, lb.amask, lb.axis, lb.tmask, lb.tvalid, lb.pairs, lb.pmask, lb.rg,
                         lb.n_tors_vina])
@@ -52,7 +57,8 @@ def dock_screen(receptor, box, ligands, cfg=None, device="cuda", seed=0, batch=N
         for k, v in st.items():
             if isinstance(v, (int, float)):
                 st_all[k] = st_all.get(k, 0) + v
-        out.extend(res)
+        for i, r in zip(idx, res):
+            out[i] = r
     if stats is not None:
         stats.update(st_all)
         stats["h2d_bytes"] = stats.get("h2d_bytes", 0) + int(h2d)

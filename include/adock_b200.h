@@ -121,11 +121,13 @@ typedef struct {
     int prop_k;
     unsigned long long* prop_stats; /* dev [4] or NULL: proposed, proposed+accepted, plain, plain+accepted */
     /* training-data log (NULL = off): each accepted improving move appends features [288] (BF16) of the pre-move
-     * state and the move [32] (translation 3, rotation vector 3, torsions 20, torsion count) while *log_n < cap */
+     * state and that state [32] (t 3, q 4, torsions 20, torsion count at 27, chain index at 28) while
+     * *log_n < cap; the training target (the move to the chain's final best state) is formed after the run */
     void* log_x;
     float* log_y;
     int* log_n;
     int log_cap;
+    float prop_frac;           /* with proposals: fraction of steps that take the learned move (<= 0 or >= 1: all) */
 } adock_mc_args_t;
 
 /* ------------------------------------------------------------------------------------------------ misc */

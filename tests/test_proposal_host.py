@@ -1,0 +1,64 @@
+"""Host-side logic of the learned proposal: the training targets built from the MC kernel's state log."""
+import math
+
+import numpy as np
+import torch
+
+from adock_b200.proposal import moves_to
+
+
+def _qmul(a, b):
+    aw, ax, ay, az = a
+    bw, bx, by, bz = b
+    return np.array([aw * bw - ax * bx - ay * by - az * bz, aw * bx + ax * bw + ay * bz - az * by,
+                     aw * by - ax * bz + ay * bw + az * bx, aw * bz + ax * by - ay * bx + az * bw])
+
+
+def _rotvec_quat(r):
+    ang = np.linalg.norm(r)
+    if ang < 1e-12:
+        return np.array([1.0, 0, 0, 0])
+    return np.concatenate([[math.cos(ang / 2)], math.sin(ang / 2) * r / ang])
+
+
+def test_moves_to_reaches_target():
+    g = torch.Generator().manual_seed(3)
+    n = 64
+    states = torch.zeros(n, 32)
+    states[:, :3] = torch.randn(n, 3, generator=g) * 3
+    q = torch.randn(n, 4, generator=g)
+    states[:, 3:7] = q / q.norm(dim=1, keepdim=True)
+    nt = torch.randint(0, 21, (n,), generator=g)
+    th = (torch.rand(n, 20, generator=g) * 2 - 1) * math.pi
+    th[torch.arange(20)[None, :] >= nt[:, None]] = 0
+    states[:, 7:27] = th
+    states[:, 27] = nt.float()
+    states[:, 28] = torch.arange(n).float()
+    target = torch.zeros(n, 7 + 24)
+    target[:, :3] = torch.randn(n, 3, generator=g) * 3
+    qt = torch.randn(n, 4, generator=g)
+    target[:, 3:7] = qt / qt.norm(dim=1, keepdim=True)
+    target[:, 7:] = (torch.rand(n, 24, generator=g) * 2 - 1) * 3 * math.pi
+    y = moves_to(states, target).double().numpy()
+    S, T = states.double().numpy(), target.double().numpy()
+    for i in range(n):
+        assert np.allclose(S[i, :3] + y[i, :3], T[i, :3], atol=1e-5)
+        assert np.linalg.norm(y[i, 3:6]) <= math.pi + 1e-5    # shortest rotation
+        qn = _qmul(_rotvec_quat(y[i, 3:6]), S[i, 3:7])
+        assert min(np.abs(qn - T[i, 3:7]).max(), np.abs(qn + T[i, 3:7]).max()) < 1e-4
+        k = int(nt[i])
+        d = y[i, 6:6 + k]
+        assert np.all(np.abs(d) <= math.pi + 1e-5)
+        diff = S[i, 7:7 + k] + d - T[i, 7:7 + k]
+        assert np.allclose(np.remainder(diff + math.pi, 2 * math.pi) - math.pi, 0, atol=1e-4)
+        assert np.all(y[i, 6 + k:26] == 0) and y[i, 26] == k and np.all(y[i, 27:] == 0)
+
+
+def test_moves_to_identity_is_zero():
+    states = torch.zeros(4, 32)
+    states[:, 3] = 1.0
+    states[:, 27] = 5
+    target = torch.zeros(4, 27)
+    target[:, 3] = 1.0
+    y = moves_to(states, target)
+    assert torch.all(y[:, :26] == 0) and torch.all(y[:, 26] == 5)
