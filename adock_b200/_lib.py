@@ -68,7 +68,7 @@ _SIGS = {
     "adock_mc_noalloc_scratch_bytes": ([I, I, I, I], ctypes.c_size_t),
     "adock_mc_noalloc": ([SP(Ligands), SP(Grids), SP(SF), SP(Receptors), SP(McArgs), P], I),
     "adock_prop_features": ([SP(Ligands), SP(Work), SP(Grids), SP(SF), P, I, P, P, P], I),
-    "adock_prop_sample": ([SP(Ligands), SP(Work), P, P, I, P, I, ctypes.c_ulonglong, I, P, P], I),
+    "adock_prop_sample": ([SP(Ligands), SP(Work), P, P, I, P, P, I, I, ctypes.c_ulonglong, I, P, P], I),
     "adock_gemm_bf16": ([I, I, I, P, ctypes.c_longlong, ctypes.c_longlong, P, ctypes.c_longlong, ctypes.c_longlong, P,
                          ctypes.c_longlong, F, P, I, P, P, ctypes.c_longlong, P], I),
     "adock_mlp_nll": ([P, P, I, P, P, P], I),

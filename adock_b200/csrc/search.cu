@@ -192,29 +192,43 @@ __global__ void __launch_bounds__(256) neighbours_kernel(const __grid_constant__
 }
 
 // ------------------------------------------------------------------------------------------ proposal sampling
-// moves[c, k, d] = mean[c, d] + max(exp(clamp(log_sd[c, d], -4, 2)), floor_d) * z, z ~ N(0, 1) by Box-Muller on the counter-based
-// stream (seed, chain id, 64 * segment + k, 2 d / 2 d + 1); torsion entries past the ligand's count are 0.
+// One thread per (chain c, slot kk): move d = mean[c, d] + max(exp(clamp(log_sd[c, d], -4, 2)), floor_d) * z with
+// z ~ N(0, 1) by Box-Muller on the counter-based stream (seed, chain id, 64 * segment + kk, 2 d / 2 d + 1), applied
+// to the chain's state: t + d[0:3], exp(d[3:6]) q, theta + d[6:26] below the torsion count (theta kept above it).
+// The floors on the spread (0.5 A, 0.25 rad, 0.5 rad) keep the proposals exploring.
 __global__ void prop_sample_kernel(const int4* info, const int* chain_lig, const int* chain_id, int n,
-                                   const float* out, int k, unsigned long long seed, int segment, float* moves) {
+                                   const float* out, const float* state, int SD, int k, unsigned long long seed,
+                                   int segment, float* targets) {
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (long long)n * k * PROP_MOVE) return;
-    const int d = (int)(idx % PROP_MOVE);
-    const int kk = (int)((idx / PROP_MOVE) % k);
-    const int c = (int)(idx / ((long long)PROP_MOVE * k));
+    if (idx >= (long long)n * k) return;
+    const int kk = (int)(idx % k);
+    const int c = (int)(idx / k);
     const int nt = info[chain_lig[c]].y;
-    float v = 0.f;
-    if (d < 26 && (d < 6 || d - 6 < nt)) {
-        const int cid = chain_id[c], step = 64 * segment + kk;
-        const float u1 = fmaxf(uniform01(seed, cid, step, 2 * d), 1e-7f);
-        const float u2 = uniform01(seed, cid, step, 2 * d + 1);
-        const float z = sqrtf(-2.f * __logf(u1)) * __cosf(6.28318531f * u2);
-        const float mu = out[(long long)c * 64 + d];
-        const float ls = fminf(fmaxf(out[(long long)c * 64 + 32 + d], -4.f), 2.f);
-        // floors on the spread (0.5 A, 0.25 rad, 0.5 rad) keep the sampled moves exploring
-        const float floor_sd = d < 3 ? 0.5f : (d < 6 ? 0.25f : 0.5f);
-        v = mu + fmaxf(__expf(ls), floor_sd) * z;
+    const int cid = chain_id[c], step = 64 * segment + kk;
+    const float* o = out + (long long)c * 64;
+    const float* s = state + (long long)c * SD;
+    float d[26];
+#pragma unroll
+    for (int j = 0; j < 26; ++j) {
+        d[j] = 0.f;
+        if (j < 6 || j - 6 < nt) {
+            const float u1 = fmaxf(uniform01(seed, cid, step, 2 * j), 1e-7f);
+            const float u2 = uniform01(seed, cid, step, 2 * j + 1);
+            const float z = sqrtf(-2.f * __logf(u1)) * __cosf(6.28318531f * u2);
+            const float ls = fminf(fmaxf(o[32 + j], -4.f), 2.f);
+            const float floor_sd = j < 3 ? 0.5f : (j < 6 ? 0.25f : 0.5f);
+            d[j] = o[j] + fmaxf(__expf(ls), floor_sd) * z;
+        }
     }
-    moves[idx] = v;
+    float* y = targets + idx * PROP_MOVE;
+    y[0] = s[0] + d[0]; y[1] = s[1] + d[1]; y[2] = s[2] + d[2];
+    float q[4] = {s[3], s[4], s[5], s[6]};
+    quat_apply_rotvec(q, d[3], d[4], d[5]);
+    y[3] = q[0]; y[4] = q[1]; y[5] = q[2]; y[6] = q[3];
+#pragma unroll
+    for (int t = 0; t < 20; ++t) y[7 + t] = (7 + t < SD) ? s[7 + t] + (t < nt ? d[6 + t] : 0.f) : 0.f;
+#pragma unroll
+    for (int t = 27; t < PROP_MOVE; ++t) y[t] = 0.f;
 }
 
 // ------------------------------------------------------------------------------------------ host side
@@ -499,16 +513,17 @@ extern "C" int adock_prop_features(const adock_ligands_t* lig, const adock_work_
 }
 
 extern "C" int adock_prop_sample(const adock_ligands_t* lig, const adock_work_t* work, const int* chain_lig,
-                                 const int* chain_id, int n, const float* net_out, int k, unsigned long long seed,
-                                 int segment, float* moves, void* stream) {
+                                 const int* chain_id, int n, const float* net_out, const float* state, int SD, int k,
+                                 unsigned long long seed, int segment, float* targets, void* stream) {
     ADOCK_CHECK_ARG(lig && work && work->info, "null argument");
-    ADOCK_CHECK_ARG(n >= 0 && k >= 1, "n must be >= 0 and k >= 1");
+    ADOCK_CHECK_ARG(n >= 0 && k >= 1 && k <= 64, "n must be >= 0 and k in [1, 64]");
+    ADOCK_CHECK_ARG(SD >= 7, "SD must be >= 7");
     if (n == 0) return ADOCK_OK;
-    ADOCK_CHECK_ARG(chain_lig && chain_id && net_out && moves, "null array argument");
-    const long long total = (long long)n * k * PROP_MOVE;
-    const unsigned blocks = (unsigned)((total + 255) / 256);
-    prop_sample_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>((const int4*)work->info, chain_lig, chain_id, n, net_out,
-                                                                 k, seed, segment, moves);
+    ADOCK_CHECK_ARG(chain_lig && chain_id && net_out && state && targets, "null array argument");
+    const long long total = (long long)n * k;
+    const unsigned blocks = (unsigned)((total + 127) / 128);
+    prop_sample_kernel<<<blocks, 128, 0, (cudaStream_t)stream>>>((const int4*)work->info, chain_lig, chain_id, n,
+                                                                 net_out, state, SD, k, seed, segment, targets);
     ADOCK_CUDA(cudaGetLastError());
     return ADOCK_OK;
 }

@@ -695,12 +695,10 @@ __global__ void __launch_bounds__(128, MINB) mc_kernel(const __grid_constant__ S
             const bool use_prop = M.prop && prop_fail < PROP_FAIL_MAX &&
                                   (M.prop_frac >= 1.f || uniform01(M.seed, cid, sg, 3) < M.prop_frac);
             if (use_prop) {
+                // the proposed target state (drawn around the state the network read at the segment start)
                 const float* mv = M.prop + ((long long)ch * M.prop_k + (st % M.prop_k)) * PROP_MOVE;
-                if (lane == 0) {
-                    x[0] += mv[0]; x[1] += mv[1]; x[2] += mv[2];
-                    quat_apply_rotvec(x + 3, mv[3], mv[4], mv[5]);
-                }
-                for (int k = lane; k < c.nt && k < 20; k += 32) x[7 + k] += mv[6 + k];
+                if (lane < 7) x[lane] = mv[lane];
+                for (int k = lane; k < c.nt && k < 20; k += 32) x[7 + k] = mv[7 + k];
             } else {
                 const int nm = 2 + c.nt;
                 const int which = min((int)(uniform01(M.seed, cid, sg, 0) * nm), nm - 1);

@@ -152,16 +152,20 @@ class B200KernelProblem:
                       _lib.ptr(st), _lib.ptr(out), _lib.stream_ptr())
         return out
 
-    def prop_sample(self, chain_lig, chain_id, net_out, k, seed, segment):
-        """Moves [N, k, 32] drawn from the network's Gaussian (net_out [N, 64])."""
+    def prop_sample(self, chain_lig, chain_id, net_out, state, k, seed, segment):
+        """Target states [N, k, 32] (t, q, torsions 0..19) drawn from the network's Gaussian (net_out [N, 64]) over
+        moves from the states state [N, SD] the network read."""
         N = net_out.shape[0]
-        moves = torch.empty(N, k, 32, device=self.device)
+        targets = torch.empty(N, k, 32, device=self.device)
         cl, ci = self._i32(chain_lig), self._i32(chain_id)
         no = net_out.float().contiguous()
+        st = state.float().contiguous()
+        assert st.shape == (N, self.SD)
         with torch.cuda.device(self.device):
-            _lib.call("adock_prop_sample", self.c_lig, self.c_work, _lib.ptr(cl), _lib.ptr(ci), N, _lib.ptr(no), int(k),
-                      int(seed) & 0xFFFFFFFFFFFFFFFF, int(segment), _lib.ptr(moves), _lib.stream_ptr())
-        return moves
+            _lib.call("adock_prop_sample", self.c_lig, self.c_work, _lib.ptr(cl), _lib.ptr(ci), N, _lib.ptr(no),
+                      _lib.ptr(st), self.SD, int(k), int(seed) & 0xFFFFFFFFFFFFFFFF, int(segment), _lib.ptr(targets),
+                      _lib.stream_ptr())
+        return targets
 
     def run_mc(self, chain_lig, chain_id, cur, cur_e, best, best_e, init_opt, mc_steps, bfgs_iters, temp,
                amp_pos, amp_rot, seed, step_offset, exact=False, nbr=None, nbr_n=None, order=None, variant=None,

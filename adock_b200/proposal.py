@@ -221,16 +221,18 @@ def _best_per_ligand(best_e, L, M):
     return best_e.view(L, M).min(1).values
 
 
-def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(250, 500, 1000, 2000),
-               ref_steps=8000, train_steps=500, log_cap=2_000_000, epochs=3, prop_k=8, seed=0, log=None):
+def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(125, 250, 500, 1000, 2000),
+               ref_steps=8000, train_steps=500, log_cap=2_000_000, epochs=3, learned=(("learned_f16", 32, 0.5),),
+               seed=0, log=None):
     """Learned proposal vs plain MC at equal step budget (config-3 style evaluation).
 
     1. Training data: plain FP32 search (Stage-A starts, ``train_steps`` MC steps) on ``train_ligs`` with the
        move log on; the network is trained on it (``epochs`` of Adam).
     2. Reference: plain FP32 search with ``ref_steps`` steps on the held-out ``eval_ligs``; E_ref(l) = the lowest
        best energy over the ligand's chains (also over all runs below, so gaps are >= 0).
-    3. For each budget S: plain FP32, plain FP16 and learned FP16 (proposals, plain fallback) from the same
-       Stage-A starts; gap(l) = E(l) - E_ref(l); reported: median gap and ligands/s of Stage A + MC.
+    3. For each budget S: plain FP32, plain FP16 and each learned FP16 variant (name, segment length prop_k,
+       learned fraction prop_frac; proposals with plain fallback) from the same Stage-A starts;
+       gap(l) = E(l) - E_ref(l); reported: median and mean gap, ligands/s of Stage A + MC, evaluations per step.
     """
     dev = torch.device(device)
     from . import params
@@ -259,8 +261,11 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(25
     probs["f16"] = (probs["f32"][0], type(probs["f32"][1])(probs["f32"][0], grid_dtype="f16"))
     L = len(eval_ligs)
 
+    variants = {name: (k, frac) for name, k, frac in learned}
+
     def run(method, steps):
         prob, kp = probs["f16" if method != "plain_f32" else "f32"]
+        ev0 = int(kp.evals[0])
         cfg = params.workload_preset(chains, steps)
         cfg["autotune"] = False
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
@@ -269,18 +274,21 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(25
         best = cur.clone()
         ce, be = torch.zeros(cur.shape[0], device=dev), torch.full((cur.shape[0],), float("inf"), device=dev)
         st = {}
-        if method == "learned_f16":
-            run_mc_segments(kp, net, cl, ci, cur, ce, best, be, cfg, seed + 3, prop_k=prop_k, stats=st)
+        if method in variants:
+            k, frac = variants[method]
+            run_mc_segments(kp, net, cl, ci, cur, ce, best, be, cfg, seed + 3, prop_k=k, prop_frac=frac, stats=st)
         else:
             kp.run_mc(cl, ci, cur, ce, best, be, True, steps, cfg["bfgs_iters"], cfg["mc_temperature"],
                       cfg["mc_amp_pos"], cfg["mc_amp_rot"], seed + 3, 0)
         ev[1].record()
         torch.cuda.synchronize(dev)
+        st["evals_per_step"] = (int(kp.evals[0]) - ev0) / (cur.shape[0] * steps)
         return _best_per_ligand(be, L, chains), ev[0].elapsed_time(ev[1]), st
 
     ref, ref_ms, _ = run("plain_f32", ref_steps)
     results = {}
-    for m in ("plain_f32", "plain_f16", "learned_f16"):
+    out["learned_variants"] = {n: {"prop_k": k, "prop_frac": f} for n, (k, f) in variants.items()}
+    for m in ("plain_f32", "plain_f16", *variants):
         for S in budgets:
             results[(m, S)] = run(m, S)
     floor = ref.clone()
@@ -301,33 +309,34 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(25
         out.setdefault("at_target_gap", {})[m] = ({"steps": ok[0]["steps"], "ligands_per_s": ok[0]["ligands_per_s"]}
                                                   if ok else None)
     a = out["at_target_gap"]
-    if a.get("learned_f16") and a.get("plain_f32"):
-        out["speedup_at_equal_gap"] = a["learned_f16"]["ligands_per_s"] / a["plain_f32"]["ligands_per_s"]
+    for m in variants:
+        if a.get(m) and a.get("plain_f32"):
+            out[f"speedup_at_equal_gap_{m}"] = a[m]["ligands_per_s"] / a["plain_f32"]["ligands_per_s"]
     # the same at a fixed median-gap bar of 0.1 kcal/mol (the accuracy bar of the screening comparison)
     for m, rs in rows.items():
         ok = [r for r in rs if r["median_gap"] <= 0.1]
         out.setdefault("at_gap_0.1", {})[m] = ({"steps": ok[0]["steps"], "ligands_per_s": ok[0]["ligands_per_s"]}
                                                if ok else None)
     b = out["at_gap_0.1"]
-    for m in ("plain_f16", "learned_f16"):
+    for m in ("plain_f16", *variants):
         if b.get(m) and b.get("plain_f32"):
             out[f"speedup_at_gap_0.1_{m}"] = b[m]["ligands_per_s"] / b["plain_f32"]["ligands_per_s"]
     return out
 
 
-def run_mc_segments(kp, net, chain_lig, chain_id, cur, cur_e, best, best_e, cfg, seed, prop_k=8, init_opt=True,
+def run_mc_segments(kp, net, chain_lig, chain_id, cur, cur_e, best, best_e, cfg, seed, prop_k=32, init_opt=True,
                     stats=None, prop_frac=0.5):
     """MC with learned proposals: the run is cut into segments of prop_k steps; before each segment the network
-    reads every chain's current state and draws prop_k moves per chain (adock_prop_sample); the MC kernel applies
-    them in order; a step takes the learned move with probability prop_frac, else the plain random move (and
-    plain MC after 8 consecutive rejections of learned moves)."""
+    reads every chain's current state and draws prop_k target states per chain around it (adock_prop_sample); a
+    step proposes the next of them with probability prop_frac, else it takes the plain random move (and plain MC
+    after 8 consecutive rejections of learned proposals)."""
     steps = cfg["mc_steps"]
     pst = torch.zeros(4, dtype=torch.int64, device=kp.device)
     for sg in range(math.ceil(steps / prop_k)):
         k = min(prop_k, steps - sg * prop_k)
         feat = kp.prop_features(chain_lig, cur)
         out = net.forward(feat)
-        moves = kp.prop_sample(chain_lig, chain_id, out, k, seed ^ 0x5EEDBA5E, sg)
+        moves = kp.prop_sample(chain_lig, chain_id, out, cur, k, seed ^ 0x5EEDBA5E, sg)
         kp.run_mc(chain_lig, chain_id, cur, cur_e, best, best_e, init_opt and sg == 0, k, cfg["bfgs_iters"],
                   cfg["mc_temperature"], cfg["mc_amp_pos"], cfg["mc_amp_rot"], seed, sg * prop_k, prop=moves,
                   prop_stats=pst, prop_frac=prop_frac)

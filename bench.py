@@ -49,6 +49,8 @@ def _args():
     ap.add_argument("--ab", action="store_true", help="learned proposal vs plain MC at equal step budget")
     ap.add_argument("--ab-train", type=int, default=256, help="fresh ligands for the proposal's training data")
     ap.add_argument("--ab-eval", type=int, default=256, help="held-out ligands for the A/B comparison")
+    ap.add_argument("--ab-variants", default="learned_f16:32:0.5",
+                    help="learned variants name:segment_steps:learned_fraction, comma separated")
     return ap.parse_args()
 
 
@@ -318,7 +320,8 @@ def run_ours(args, rank, world, local_rank):
         from adock_b200.proposal import ab_compare
         train = synth.ligand_set(args.ab_train, (10, 60), (0, 15), seed0=100_000)
         held = synth.ligand_set(args.ab_eval, (10, 60), (0, 15), seed0=200_000)
-        out["learned_proposal"] = ab_compare(rec, train, held, device=dev)
+        variants = [(v.split(":")[0], int(v.split(":")[1]), float(v.split(":")[2])) for v in args.ab_variants.split(",")]
+        out["learned_proposal"] = ab_compare(rec, train, held, device=dev, learned=variants)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = _cpu_baseline(ligs, rec, cfg)
     return out

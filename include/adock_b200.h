@@ -115,8 +115,9 @@ typedef struct {
     int* queue;                /* dev, 1 int work counter, zeroed by the call on `stream` */
     unsigned long long* evals; /* dev, 2 counters (accumulated): energy evaluations, atom evaluations; or NULL */
     int variant;               /* launch variant (0 = default; 1-3 = 4, 6, 8 resident blocks per SM), autotuned */
-    /* learned proposal (no reference counterpart): moves [N, prop_k, 32] for the launch's steps (NULL = plain MC);
-     * after 8 consecutive rejections of proposed moves a chain falls back to plain MC until a move is accepted */
+    /* learned proposal (no reference counterpart): target states [N, prop_k, 32] from adock_prop_sample for the
+     * launch's steps (NULL = plain MC); a learned step proposes its target state (torsions past 20 unchanged);
+     * after 8 consecutive rejections of proposed states a chain falls back to plain MC until a move is accepted */
     const float* prop;
     int prop_k;
     unsigned long long* prop_stats; /* dev [4] or NULL: proposed, proposed+accepted, plain, plain+accepted */
@@ -204,11 +205,14 @@ int adock_rescore64(const adock_ligands_t* lig, const adock_work_t* work, const 
 int adock_prop_features(const adock_ligands_t* lig, const adock_work_t* work, const adock_grids_t* grids,
                         const adock_sf_t* sf, const int* chain_lig, int n, const float* state, void* feat,
                         void* stream);
-/* Moves [n, k, 32] (dev) drawn from the network output [n, 64]: move = mean + exp(log_sd) * z, z standard normal
- * from a counter-based stream of (seed, chain_id, segment, slot); torsion entries past a ligand's count are 0. */
+/* Proposed target states [n, k, 32] (dev; t 3, q 4, torsions 20, rest 0) drawn from the network output [n, 64]
+ * around the states state [n, SD] the network read: move = mean + max(exp(log_sd), floor) * z, z standard normal
+ * from a counter-based stream of (seed, chain_id, segment, slot), applied to the state (translation added,
+ * rotation vector composed on the left of q, torsion deltas added; torsions past a ligand's count keep their
+ * value). k <= 64. */
 int adock_prop_sample(const adock_ligands_t* lig, const adock_work_t* work, const int* chain_lig, const int* chain_id,
-                      int n, const float* net_out, int k, unsigned long long seed, int segment, float* moves,
-                      void* stream);
+                      int n, const float* net_out, const float* state, int SD, int k, unsigned long long seed,
+                      int segment, float* targets, void* stream);
 /* C[M,N] = A[M,K] B[K,N] on the tensor cores (BF16 operands at any strides, FP32 accumulation); epilogue
  * C = acc + beta C + bias, optional pre-activation copy, optional SiLU (act = 1), optional BF16 copy Cb. */
 int adock_gemm_bf16(int M, int N, int K, const void* A, long long sAm, long long sAk, const void* B, long long sBk,
