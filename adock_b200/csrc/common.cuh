@@ -98,24 +98,23 @@ __host__ inline PairPrm make_pair_prm(const float* prm) {
 #define PF_HYD 1
 #define PF_HB 2
 
+// Branch-free: the repulsion acts below rep_off and the hydrophobic / H-bond terms are ramps from 1 (d <= good)
+// to 0 (d >= bad); written as clamps and selects, which add exactly 0 where the piecewise form adds nothing.
 __device__ __forceinline__ float pair_energy(float r, float rsum, int flags, const PairPrm& p, float& de) {
-    float d = r - rsum;
-    float u1 = (d - p.g1_off) * p.g1_inv, g1 = __expf(-u1 * u1);
-    float u2 = (d - p.g2_off) * p.g2_inv, g2 = __expf(-u2 * u2);
+    const float d = r - rsum;
+    const float u1 = (d - p.g1_off) * p.g1_inv, g1 = __expf(-u1 * u1);
+    const float u2 = (d - p.g2_off) * p.g2_inv, g2 = __expf(-u2 * u2);
     float e = p.w_g1 * g1 + p.w_g2 * g2;
     de = p.w_g1 * (-2.f * u1 * p.g1_inv) * g1 + p.w_g2 * (-2.f * u2 * p.g2_inv) * g2;
-    float dr = d - p.rep_off;
-    if (dr < 0.f) { e += p.w_rep * dr * dr; de += p.w_rep * 2.f * dr; }
-    if (flags & PF_HYD) {
-        float v = (p.hyd_bad - d) * p.hyd_inv;
-        if (v >= 1.f) e += p.w_hyd;
-        else if (v > 0.f) { e += p.w_hyd * v; de -= p.w_hyd * p.hyd_inv; }
-    }
-    if (flags & PF_HB) {
-        float v = (p.hb_bad - d) * p.hb_inv;
-        if (v >= 1.f) e += p.w_hb;
-        else if (v > 0.f) { e += p.w_hb * v; de -= p.w_hb * p.hb_inv; }
-    }
+    const float dr = fminf(d - p.rep_off, 0.f);
+    e += p.w_rep * dr * dr;
+    de += p.w_rep * 2.f * dr;
+    const float wh = (flags & PF_HYD) ? p.w_hyd : 0.f, wb = (flags & PF_HB) ? p.w_hb : 0.f;
+    const float vh = (p.hyd_bad - d) * p.hyd_inv, vb = (p.hb_bad - d) * p.hb_inv;
+    e += wh * fminf(fmaxf(vh, 0.f), 1.f);
+    e += wb * fminf(fmaxf(vb, 0.f), 1.f);
+    de -= (vh > 0.f && vh < 1.f) ? wh * p.hyd_inv : 0.f;
+    de -= (vb > 0.f && vb < 1.f) ? wb * p.hb_inv : 0.f;
     return e;
 }
 

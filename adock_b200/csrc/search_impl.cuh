@@ -114,8 +114,8 @@ struct WSLayout {
     __host__ __device__ WSLayout(int AM, int KM) {
         const int DM = 6 + KM, SD = 7 + KM;
         int o = 0;
-        X = o; o += 4 * AM;
-        FF = o; o += 4 * AM;
+        X = o; o += 3 * AM;    // world coordinates, [3][AM] (x, y, z arrays)
+        FF = o; o += 3 * AM;   // forces, [3][AM]
         ap = o; o += 4 * KM;
         au = o; o += 4 * KM;
         tp = o; o += 4 * KM;
@@ -245,19 +245,24 @@ __device__ __forceinline__ float trilinear(const GT* G, int ny, int nz, const fl
     return e;
 }
 
-// Intra-ligand pair term of one scheduled slot: energy, and the force added into both atoms' slots.
-__device__ __forceinline__ float pair_slot(int2 pr, const float4* X, float4* FF, const PairPrm& pp) {
+// Intra-ligand pair term of one scheduled slot: energy, and the force added into both atoms' entries. Positions X
+// and forces F are three arrays of AM floats each (x, y, z), so that 32 lanes touching 32 different atoms hit 32
+// different shared-memory banks (a float4 per atom would put the x components of 32 atoms on 8 banks).
+template <int AM>
+__device__ __forceinline__ float pair_slot(int2 pr, const float* X, float* F, const PairPrm& pp) {
     if (pr.x < 0) return 0.f;
     const int i = pr.x & 0xff, j = (pr.x >> 8) & 0xff, fl = pr.x >> 16;
-    const float4 Xi = X[i], Xj = X[j];
-    const float rx = Xi.x - Xj.x, ry = Xi.y - Xj.y, rz = Xi.z - Xj.z;
-    const float r = sqrtf(rx * rx + ry * ry + rz * rz);
+    const float rx = X[i] - X[j], ry = X[AM + i] - X[AM + j], rz = X[2 * AM + i] - X[2 * AM + j];
+    // r and 1/r from one reciprocal square root; clamping r^2 at 1e-12 is the reference's max(r, 1e-6)
+    const float r2 = rx * rx + ry * ry + rz * rz;
+    const float rinv = rsqrtf(fmaxf(r2, 1e-12f));
+    const float r = r2 * rinv;
     if (r >= pp.cutoff) return 0.f;
     float de;
     const float e = pair_energy(r, __int_as_float(pr.y), fl, pp, de);
-    const float sc = de / fmaxf(r, 1e-6f);
-    atomicAdd(&FF[i].x, sc * rx); atomicAdd(&FF[i].y, sc * ry); atomicAdd(&FF[i].z, sc * rz);
-    atomicAdd(&FF[j].x, -sc * rx); atomicAdd(&FF[j].y, -sc * ry); atomicAdd(&FF[j].z, -sc * rz);
+    const float sc = de * rinv;
+    atomicAdd(F + i, sc * rx); atomicAdd(F + AM + i, sc * ry); atomicAdd(F + 2 * AM + i, sc * rz);
+    atomicAdd(F + j, -sc * rx); atomicAdd(F + AM + j, -sc * ry); atomicAdd(F + 2 * AM + j, -sc * rz);
     return e;
 }
 
@@ -269,8 +274,9 @@ __device__ __forceinline__ float pair_slot(int2 pr, const float4* X, float4* FF,
 template <int APL, typename GT>
 __device__ __forceinline__ float eval_eg(float* ws, const WSLayout& L, const float* s, float* g, const Chain<APL>& c,
                          const SearchParams& P, const TypeTables& tt, int lane) {
-    float4* X = (float4*)(ws + L.X);
-    float4* FF = (float4*)(ws + L.FF);
+    constexpr int AM = 32 * APL;
+    float* X = ws + L.X;     // [3][AM] world coordinates
+    float* FF = ws + L.FF;   // [3][AM] forces dE/dX
     const float4* ap = (const float4*)(ws + L.ap);
     const float4* au = (const float4*)(ws + L.au);
     float4* tp = (float4*)(ws + L.tp);
@@ -317,7 +323,9 @@ __device__ __forceinline__ float eval_eg(float* ws, const WSLayout& L, const flo
             const float X0 = R00 * px + R01 * py + R02 * pz + t0;
             const float X1 = R10 * px + R11 * py + R12 * pz + t1;
             const float X2 = R20 * px + R21 * py + R22 * pz + t2;
-            X[a] = make_float4(X0, X1, X2, 0.f);
+            X[a] = X0;
+            X[AM + a] = X1;
+            X[2 * AM + a] = X2;
             float ea, gg[3];
             if (c.exact) {
                 ea = 0.f;
@@ -334,10 +342,11 @@ __device__ __forceinline__ float eval_eg(float* ws, const WSLayout& L, const flo
                     if (r2 >= cut2) continue;
                     const int tb = c.rt[b] & 63;   // index kept inside the 64-entry type tables
                     const int fb = tt.flags[tb];
-                    const float r = sqrtf(r2);
+                    const float rinv = rsqrtf(fmaxf(r2, 1e-12f));
+                    const float r = r2 * rinv;
                     float de;
                     ea += pair_energy(r, ra + tt.radius[tb], hyd_pair(fa, fb) | hb_pair(fa, fb), P.pp, de);
-                    const float sc = de / fmaxf(r, 1e-6f);
+                    const float sc = de * rinv;
                     gg[0] += sc * rx; gg[1] += sc * ry; gg[2] += sc * rz;
                 }
             } else {
@@ -352,25 +361,35 @@ __device__ __forceinline__ float eval_eg(float* ws, const WSLayout& L, const flo
                 gg[d] += P.pen * (-2.f * lo + 2.f * hi);
             }
             e += ea;
-            FF[a] = make_float4(gg[0], gg[1], gg[2], 0.f);
+            FF[a] = gg[0];
+            FF[AM + a] = gg[1];
+            FF[2 * AM + a] = gg[2];
         }
     }
     __syncwarp();
     // intra-ligand pairs, scheduled in rounds of 32 in which an atom appears at most once (adock_prepare), so the
     // force atomics of one round do not collide; two rounds in flight per iteration
-    for (int r = 0; r < c.nrounds; r += 2) {
-        const int2 pa = c.pairs[r * 32 + lane];
-        const int2 pb = (r + 1 < c.nrounds) ? c.pairs[(r + 1) * 32 + lane] : make_int2(-1, 0);
-        e += pair_slot(pa, X, FF, P.pp);
-        e += pair_slot(pb, X, FF, P.pp);
+    // the next two rounds' records are loaded while the current two are evaluated
+    {
+        const int2 none = make_int2(-1, 0);
+        int2 pa = c.nrounds > 0 ? c.pairs[lane] : none;
+        int2 pb = c.nrounds > 1 ? c.pairs[32 + lane] : none;
+        for (int r = 0; r < c.nrounds; r += 2) {
+            const int2 qa = (r + 2 < c.nrounds) ? c.pairs[(r + 2) * 32 + lane] : none;
+            const int2 qb = (r + 3 < c.nrounds) ? c.pairs[(r + 3) * 32 + lane] : none;
+            e += pair_slot<AM>(pa, X, FF, P.pp);
+            e += pair_slot<AM>(pb, X, FF, P.pp);
+            pa = qa;
+            pb = qb;
+        }
     }
     // world torsion axes (axis atoms' current positions)
     for (int k = lane; k < c.nt; k += 32) {
         const int a0 = axs[k] & 0xffff, a1 = axs[k] >> 16;
-        const float4 A = X[a0], B = X[a1];
-        const float ux = B.x - A.x, uy = B.y - A.y, uz = B.z - A.z;
+        const float Ax = X[a0], Ay = X[AM + a0], Az = X[2 * AM + a0];
+        const float ux = X[a1] - Ax, uy = X[AM + a1] - Ay, uz = X[2 * AM + a1] - Az;
         const float nn = rsqrtf(fmaxf(ux * ux + uy * uy + uz * uz, 1e-12f));
-        tp[k] = make_float4(A.x - t0, A.y - t1, A.z - t2, 0.f);
+        tp[k] = make_float4(Ax - t0, Ay - t1, Az - t2, 0.f);
         tu[k] = make_float4(ux * nn, uy * nn, uz * nn, 0.f);
     }
     __syncwarp();
@@ -386,10 +405,10 @@ __device__ __forceinline__ float eval_eg(float* ws, const WSLayout& L, const flo
             const bool all = (k == c.nt);
             for (int a = chunk; a < c.na; a += C) {
                 if (all || (smk[a] & bit)) {
-                    const float4 F = FF[a], Xa = X[a];
-                    const float dx = Xa.x - t0, dy = Xa.y - t1, dz = Xa.z - t2;
-                    S0 += F.x; S1 += F.y; S2 += F.z;
-                    T0 += dy * F.z - dz * F.y; T1 += dz * F.x - dx * F.z; T2 += dx * F.y - dy * F.x;
+                    const float Fx = FF[a], Fy = FF[AM + a], Fz = FF[2 * AM + a];
+                    const float dx = X[a] - t0, dy = X[AM + a] - t1, dz = X[2 * AM + a] - t2;
+                    S0 += Fx; S1 += Fy; S2 += Fz;
+                    T0 += dy * Fz - dz * Fy; T1 += dz * Fx - dx * Fz; T2 += dx * Fy - dy * Fx;
                 }
             }
         }
@@ -416,10 +435,10 @@ __device__ __forceinline__ float eval_eg(float* ws, const WSLayout& L, const flo
             const uint32_t bit = all ? 0u : (1u << k);
             for (int a = 0; a < c.na; ++a) {
                 if (all || (smk[a] & bit)) {
-                    const float4 F = FF[a], Xa = X[a];
-                    const float dx = Xa.x - t0, dy = Xa.y - t1, dz = Xa.z - t2;
-                    S0 += F.x; S1 += F.y; S2 += F.z;
-                    T0 += dy * F.z - dz * F.y; T1 += dz * F.x - dx * F.z; T2 += dx * F.y - dy * F.x;
+                    const float Fx = FF[a], Fy = FF[AM + a], Fz = FF[2 * AM + a];
+                    const float dx = X[a] - t0, dy = X[AM + a] - t1, dz = X[2 * AM + a] - t2;
+                    S0 += Fx; S1 += Fy; S2 += Fz;
+                    T0 += dy * Fz - dz * Fy; T1 += dz * Fx - dx * Fz; T2 += dx * Fy - dy * Fx;
                 }
             }
             if (all) {
