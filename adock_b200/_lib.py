@@ -71,6 +71,9 @@ _SIGS = {
     "adock_prop_sample": ([SP(Ligands), SP(Work), P, P, I, P, P, I, I, ctypes.c_ulonglong, I, P, P], I),
     "adock_gemm_bf16": ([I, I, I, P, ctypes.c_longlong, ctypes.c_longlong, P, ctypes.c_longlong, ctypes.c_longlong, P,
                          ctypes.c_longlong, F, P, I, P, P, ctypes.c_longlong, P], I),
+    "adock_gemm_bf16_mma": ([I, I, I, P, ctypes.c_longlong, ctypes.c_longlong, P, ctypes.c_longlong,
+                             ctypes.c_longlong, P, ctypes.c_longlong, F, P, I, P, P, ctypes.c_longlong, P], I),
+    "adock_gemm_status": ([], I),
     "adock_mlp_nll": ([P, P, I, P, P, P], I),
     "adock_silu_backward": ([P, P, ctypes.c_longlong, P, P], I),
     "adock_bias_grad": ([P, I, I, P, P], I),
@@ -83,7 +86,7 @@ _lib = None
 _lock = threading.Lock()
 # kernel launches issued through call() (each launching entry point issues one kernel)
 LAUNCHES = [0]
-_NO_LAUNCH = {"adock_version", "adock_last_error", "adock_mc_noalloc_scratch_bytes"}
+_NO_LAUNCH = {"adock_version", "adock_last_error", "adock_mc_noalloc_scratch_bytes", "adock_gemm_status"}
 
 
 def load():

@@ -206,8 +206,11 @@ def dock_problem_kernel(prob, boxes_c, boxes_s, cfg, seed=0, log=None, stats=Non
                 active = active & (stall < es_rounds)
             if log is not None:
                 log(f"segment {sg}: active {int(active.sum())}/{L}, best E mean {glob.mean().item():.3f}")
+    mc_counts = None
     if ev is not None:
         ev[1].record()
+        if hasattr(kp, "evals"):
+            mc_counts = kp.evals.clone()   # counters of the MC phase alone (no host sync)
     _mark("mc")
     if cfg.get("final_bfgs_iters", 0) > 0:
         fe = torch.zeros(N, device=dev)
@@ -240,6 +243,9 @@ def dock_problem_kernel(prob, boxes_c, boxes_s, cfg, seed=0, log=None, stats=Non
         if hasattr(kp, "evals"):
             ev_ = kp.evals.tolist()
             stats["evals"], stats["atom_evals"] = int(ev_[0]), int(ev_[1])
+        if mc_counts is not None:
+            mc_ = mc_counts.tolist()
+            stats["mc_evals"], stats["mc_atom_evals"] = int(mc_[0]), int(mc_[1])
     return res
 
 

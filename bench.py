@@ -256,8 +256,8 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize(dev)
         step_ms.append(e0.elapsed_time(e1))
         mc_ms.append(st["mc_ms"])
-        evals += st["evals"]
-        atom_evals += st["atom_evals"]
+        evals += st["mc_evals"]            # the MC phase (the timed dominant launch) alone
+        atom_evals += st["mc_atom_evals"]
     barrier()
     clk = clocks.stop()
     launches = _lib.LAUNCHES[0] - launches0

@@ -213,11 +213,20 @@ int adock_prop_features(const adock_ligands_t* lig, const adock_work_t* work, co
 int adock_prop_sample(const adock_ligands_t* lig, const adock_work_t* work, const int* chain_lig, const int* chain_id,
                       int n, const float* net_out, const float* state, int SD, int k, unsigned long long seed,
                       int segment, float* targets, void* stream);
-/* C[M,N] = A[M,K] B[K,N] on the tensor cores (BF16 operands at any strides, FP32 accumulation); epilogue
- * C = acc + beta C + bias, optional pre-activation copy, optional SiLU (act = 1), optional BF16 copy Cb. */
+/* C[M,N] = A[M,K] B[K,N] on the 5th-generation tensor cores (tcgen05.mma, accumulator in tensor memory; BF16
+ * operands at any strides, FP32 accumulation); epilogue C = acc + beta C + bias, optional pre-activation copy,
+ * optional SiLU (act = 1), optional BF16 copy Cb. */
 int adock_gemm_bf16(int M, int N, int K, const void* A, long long sAm, long long sAk, const void* B, long long sBk,
                     long long sBn, float* C, long long ldc, float beta, const float* bias, int act, float* pre,
                     void* Cb, long long ldcb, void* stream);
+/* The same product on the warp-level mma.sync tensor-core path (an independent implementation, kept to
+ * cross-check adock_gemm_bf16). */
+int adock_gemm_bf16_mma(int M, int N, int K, const void* A, long long sAm, long long sAk, const void* B,
+                        long long sBk, long long sBn, float* C, long long ldc, float beta, const float* bias, int act,
+                        float* pre, void* Cb, long long ldcb, void* stream);
+/* Device status of the tcgen05 GEMMs since the last call (synchronises): ADOCK_E_DEVICE if a CTA gave up waiting
+ * for its tensor-core work (its tile is then not written), else 0. Clears the status. */
+int adock_gemm_status(void);
 /* Gaussian NLL of moves target [B, 32] under out [B, 64]; dout (BF16 [B, 64]) = gradient of the batch mean;
  * *loss += summed NLL. */
 int adock_mlp_nll(const float* out, const float* target, int B, void* dout, float* loss, void* stream);

@@ -35,6 +35,43 @@ def test_gemm_bf16_matches_torch(dev, M, N, K, ta, tb):
         _gemm(A, sA, B, sB, M, N, K, C=C, bias=bias)
     ref = Am.float() @ Bm.float() + bias
     torch.testing.assert_close(C, ref, rtol=1e-4, atol=1e-3)
+    from adock_b200 import _lib
+    assert _lib.load().adock_gemm_status() == 0
+
+
+def _gemm_call(name, A, sA, B, sB, M, N, K, C=None, beta=0.0, bias=None, act=0, pre=None, Cb=None):
+    from adock_b200 import _lib
+    _lib.call(name, M, N, K, _lib.ptr(A), sA[0], sA[1], _lib.ptr(B), sB[0], sB[1], _lib.ptr(C),
+              N if C is not None else 0, float(beta), _lib.ptr(bias), int(act), _lib.ptr(pre), _lib.ptr(Cb),
+              N if Cb is not None else 0, _lib.stream_ptr())
+
+
+@pytest.mark.parametrize("M,N,K", [(8192, 256, 288), (300, 200, 70), (129, 65, 16), (1, 1, 1), (5, 130, 0)])
+def test_gemm_tcgen05_epilogue_matches_mma_sync(dev, M, N, K):
+    """The tcgen05 GEMM against the independent mma.sync kernel: beta accumulation, bias, pre-activation copy,
+    SiLU and the BF16 copy, on sizes that are not tile multiples (and K = 0)."""
+    from adock_b200 import _lib
+    g = torch.Generator(device=dev).manual_seed(M + 3 * N + 7 * K)
+    A = torch.randn(M, max(K, 1), device=dev, generator=g).to(torch.bfloat16)
+    B = torch.randn(max(K, 1), N, device=dev, generator=g).to(torch.bfloat16)
+    C0 = torch.randn(M, N, device=dev, generator=g)
+    bias = torch.randn(N, device=dev, generator=g)
+    out = {}
+    for name in ("adock_gemm_bf16", "adock_gemm_bf16_mma"):
+        C, pre = C0.clone(), torch.empty(M, N, device=dev)
+        Cb = torch.empty(M, N, dtype=torch.bfloat16, device=dev)
+        with torch.cuda.device(dev):
+            _gemm_call(name, A, (max(K, 1), 1), B, (N, 1), M, N, K, C=C, beta=0.5, bias=bias, act=1, pre=pre, Cb=Cb)
+        out[name] = (C, pre, Cb)
+    torch.cuda.synchronize(dev)
+    assert _lib.load().adock_gemm_status() == 0
+    ref_pre = (A[:, :K].float() @ B[:K].float() if K > 0 else torch.zeros(M, N, device=dev)) + 0.5 * C0 + bias
+    for name, (C, pre, Cb) in out.items():
+        torch.testing.assert_close(pre, ref_pre, rtol=1e-4, atol=2e-3, msg=name)
+        torch.testing.assert_close(C, torch.nn.functional.silu(ref_pre), rtol=1e-4, atol=2e-3, msg=name)
+        torch.testing.assert_close(Cb.float(), C, rtol=1e-2, atol=1e-2, msg=name)
+    a, b = out["adock_gemm_bf16"][1], out["adock_gemm_bf16_mma"][1]
+    torch.testing.assert_close(a, b, rtol=1e-5, atol=1e-4)
 
 
 def test_network_gradients_match_float64_oracle(dev):
