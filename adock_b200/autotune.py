@@ -42,9 +42,12 @@ def _save_file():
         os.replace(tmp, path)
 
 
-def tune_mc(kp, chain_lig, state, max_chains=4096, steps=4, reps=2):
+def tune_mc(kp, chain_lig, state, max_chains=16384, steps=4, reps=2):
     """Return the fastest MC launch variant for this kernel object (cached). Each variant runs ``steps`` MC steps
-    on the sample ``reps`` times from the same starts; the best time counts (variants differ by a few percent)."""
+    on the sample ``reps`` times from the same starts; the best time counts (variants differ by a few percent).
+    The sample is the whole batch up to ``max_chains`` chains: a chain's time scales with its step count, so a short
+    run over the batch has the waves and the tail of the full persistent launch (a sample of about one wave would
+    be decided by its tail instead)."""
     key = _key(kp)
     with _lock:
         if not _cache:
@@ -53,10 +56,13 @@ def tune_mc(kp, chain_lig, state, max_chains=4096, steps=4, reps=2):
             return int(_cache[key]["variant"])
     dev = kp.device
     N = state.shape[0]
-    order = kp.chain_order(chain_lig).long()
-    # the most expensive chains plus an even spread of the rest (the tail of the persistent launch matters)
-    take = order[: max_chains // 4].tolist() + order[max_chains // 4:: max(1, N // max_chains)].tolist()
-    idx = torch.tensor(sorted(set(take))[:max_chains], device=dev, dtype=torch.long)
+    if N <= max_chains:
+        idx = torch.arange(N, device=dev, dtype=torch.long)
+    else:
+        # the most expensive chains plus an even spread of the rest
+        order = kp.chain_order(chain_lig).long()
+        take = order[: max_chains // 4].tolist() + order[max_chains // 4:: max(1, N // max_chains)].tolist()
+        idx = torch.tensor(sorted(set(take))[:max_chains], device=dev, dtype=torch.long)
     cl = chain_lig[idx].to(torch.int32)
     ci = torch.arange(len(idx), device=dev, dtype=torch.int32)
     times = {}

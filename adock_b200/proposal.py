@@ -170,10 +170,23 @@ def moves_to(states, target):
     return y
 
 
-def collect(kp, chain_lig, chain_id, cur, cur_e, best, best_e, cfg, seed, cap, init_opt=True):
+def ligand_best_chain(chain_lig, best_e):
+    """Per ligand (0..max), the index of its chain with the lowest best energy (the highest index among ties;
+    -1 for a ligand without chains)."""
+    lig = chain_lig.long()
+    L = int(lig.max()) + 1
+    lo = torch.full((L,), float("inf"), device=best_e.device).scatter_reduce(0, lig, best_e, "amin")
+    idx = torch.arange(len(lig), device=best_e.device)
+    cand = torch.where(best_e <= lo[lig], idx, torch.full_like(idx, -1))
+    return torch.full((L,), -1, dtype=torch.long, device=best_e.device).scatter_reduce(0, lig, cand, "amax")
+
+
+def collect(kp, chain_lig, chain_id, cur, cur_e, best, best_e, cfg, seed, cap, init_opt=True, target="chain"):
     """Run the plain MC search on the given chains with the training-data log on; returns (X BF16 [n, 288],
     Y [n, 32]): the features of the pre-move state of each accepted improving move and, as its target, the move
-    from that state to the chain's best state at the end of the run (n <= cap)."""
+    from that state to a low-energy minimum the run found (n <= cap). target "chain": the chain's own best state
+    at the end of the run; "ligand": the best state over all chains of the chain's ligand; "both": returns
+    (X, Y_chain, Y_ligand)."""
     dev = kp.device
     lx = torch.empty(cap, IN, dtype=torch.bfloat16, device=dev)
     ly = torch.empty(cap, 32, device=dev)
@@ -182,7 +195,15 @@ def collect(kp, chain_lig, chain_id, cur, cur_e, best, best_e, cfg, seed, cap, i
               cfg["mc_temperature"], cfg["mc_amp_pos"], cfg["mc_amp_rot"], seed, 0, log=(lx, ly, ln))
     n = min(int(ln), cap)
     states = ly[:n]
-    return lx[:n], moves_to(states, best[states[:, 28].long()])
+    ch = states[:, 28].long()
+    y_chain = y_lig = None
+    if target in ("chain", "both"):
+        y_chain = moves_to(states, best[ch])
+    if target in ("ligand", "both"):
+        y_lig = moves_to(states, best[ligand_best_chain(chain_lig, best_e)[chain_lig.long()[ch]]])
+    if target == "both":
+        return lx[:n], y_chain, y_lig
+    return lx[:n], (y_chain if target == "chain" else y_lig)
 
 
 def _starts(prob, kp, cfg, seed):
@@ -246,22 +267,27 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
     best = cur.clone()
     ce, be = torch.zeros(N, device=dev), torch.full((N,), float("inf"), device=dev)
     torch.cuda.synchronize(dev)
-    X, Y = collect(kp_t, cl, ci, cur, ce, best, be, cfg_tr, seed=seed + 1, cap=log_cap)
-    net = ProposalNet(dev, seed=seed)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    loss = net.fit(X, Y, epochs=epochs, batch=4096, lr=1e-3, seed=seed, log=log)
-    e1.record()
-    torch.cuda.synchronize(dev)
-    out["train"] = {"moves": int(X.shape[0]), "epochs": epochs, "final_loss": loss, "train_ms": e0.elapsed_time(e1),
-                    "loss_untrained": float(ProposalNet(dev, seed=seed).loss_grad(X[:65536], Y[:65536])[0])}
-    del X, Y, kp_t, prob_t
+    # learned variants: (name, segment steps, learned fraction[, training target "chain" | "ligand"])
+    variants = {v[0]: (v[1], v[2], v[3] if len(v) > 3 else "chain") for v in learned}
+    X, Yc, Yl = collect(kp_t, cl, ci, cur, ce, best, be, cfg_tr, seed=seed + 1, cap=log_cap, target="both")
+    nets = {}
+    out["train"] = {"moves": int(X.shape[0]), "epochs": epochs}
+    for tgt in sorted({t for (_, _, t) in variants.values()}):
+        Y = Yc if tgt == "chain" else Yl
+        net = ProposalNet(dev, seed=seed)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        loss = net.fit(X, Y, epochs=epochs, batch=4096, lr=1e-3, seed=seed, log=log)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        nets[tgt] = net
+        out["train"][tgt] = {"final_loss": loss, "train_ms": e0.elapsed_time(e1),
+                             "loss_untrained": float(ProposalNet(dev, seed=seed).loss_grad(X[:65536], Y[:65536])[0])}
+    del X, Yc, Yl, kp_t, prob_t
     # 2./3. evaluation on held-out ligands
     probs = {"f32": _problem_for(rec, eval_ligs, dev, "f32")}
     probs["f16"] = (probs["f32"][0], type(probs["f32"][1])(probs["f32"][0], grid_dtype="f16"))
     L = len(eval_ligs)
-
-    variants = {name: (k, frac) for name, k, frac in learned}
 
     def run(method, steps):
         prob, kp = probs["f16" if method != "plain_f32" else "f32"]
@@ -275,8 +301,9 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
         ce, be = torch.zeros(cur.shape[0], device=dev), torch.full((cur.shape[0],), float("inf"), device=dev)
         st = {}
         if method in variants:
-            k, frac = variants[method]
-            run_mc_segments(kp, net, cl, ci, cur, ce, best, be, cfg, seed + 3, prop_k=k, prop_frac=frac, stats=st)
+            k, frac, tgt = variants[method]
+            run_mc_segments(kp, nets[tgt], cl, ci, cur, ce, best, be, cfg, seed + 3, prop_k=k, prop_frac=frac,
+                            stats=st)
         else:
             kp.run_mc(cl, ci, cur, ce, best, be, True, steps, cfg["bfgs_iters"], cfg["mc_temperature"],
                       cfg["mc_amp_pos"], cfg["mc_amp_rot"], seed + 3, 0)
@@ -287,7 +314,7 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
 
     ref, ref_ms, _ = run("plain_f32", ref_steps)
     results = {}
-    out["learned_variants"] = {n: {"prop_k": k, "prop_frac": f} for n, (k, f) in variants.items()}
+    out["learned_variants"] = {n: {"prop_k": k, "prop_frac": f, "target": t} for n, (k, f, t) in variants.items()}
     for m in ("plain_f32", "plain_f16", *variants):
         for S in budgets:
             results[(m, S)] = run(m, S)

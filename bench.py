@@ -50,7 +50,13 @@ def _args():
     ap.add_argument("--ab-train", type=int, default=256, help="fresh ligands for the proposal's training data")
     ap.add_argument("--ab-eval", type=int, default=256, help="held-out ligands for the A/B comparison")
     ap.add_argument("--ab-variants", default="learned_f16:32:0.5",
-                    help="learned variants name:segment_steps:learned_fraction, comma separated")
+                    help="learned variants name:segment_steps:learned_fraction[:chain|ligand training target], "
+                         "comma separated")
+    ap.add_argument("--screen", action="store_true",
+                    help="screening comparison on the 8,000-atom receptor with 8-80-atom ligands (FP16 + learned "
+                         "proposal vs plain FP32 at equal median gap)")
+    ap.add_argument("--screen-train", type=int, default=512, help="fresh ligands for the screening proposal's training")
+    ap.add_argument("--screen-eval", type=int, default=1024, help="held-out ligands of the screening comparison")
     return ap.parse_args()
 
 
@@ -262,11 +268,8 @@ def run_ours(args, rank, world, local_rank):
     clk = clocks.stop()
     launches = _lib.LAUNCHES[0] - launches0
     t_rank = sum(step_ms)
-    t_max = t_rank
-    if world > 1:
-        tt = torch.tensor([t_rank], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt)
+    from adock_b200.distributed import max_over_ranks
+    t_max = max_over_ranks(t_rank, device=dev) if world > 1 else t_rank
     value = args.ligands * world * args.steps / (t_max / 1e3)
 
     # ---- end to end through the public API from host arrays ----
@@ -289,9 +292,7 @@ def run_ours(args, rank, world, local_rank):
             assert len(res) == len(ligs) and all(len(r["affinity"]) >= 1 for r in res)
         t = sum(e2e_ms)
         if world > 1:
-            tt = torch.tensor([t], device=dev, dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t = float(tt)
+            t = max_over_ranks(t, device=dev)
         e2e = {"value": args.ligands * world * len(e2e_ms) / (t / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h)}
 
@@ -315,13 +316,28 @@ def run_ours(args, rank, world, local_rank):
            "mc_autotune": __import__("adock_b200.autotune", fromlist=["cached"]).cached()}
     if rank == 0 and world == 1 and not args.no_extras:
         out["grid_and_precision"] = _grid_and_precision(dev, ligs)
+    variants = []
+    for v in args.ab_variants.split(","):
+        f = v.split(":")
+        variants.append((f[0], int(f[1]), float(f[2])) + ((f[3],) if len(f) > 3 else ()))
     if rank == 0 and world == 1 and args.ab:
         from adock_b200 import synth
         from adock_b200.proposal import ab_compare
         train = synth.ligand_set(args.ab_train, (10, 60), (0, 15), seed0=100_000)
         held = synth.ligand_set(args.ab_eval, (10, 60), (0, 15), seed0=200_000)
-        variants = [(v.split(":")[0], int(v.split(":")[1]), float(v.split(":")[2])) for v in args.ab_variants.split(",")]
         out["learned_proposal"] = ab_compare(rec, train, held, device=dev, learned=variants)
+    if rank == 0 and world == 1 and args.screen:
+        # screening shapes: the 8,000-atom receptor (30 A box, 81^3 maps), ligands with 8-80 heavy atoms and
+        # 0-20 torsions; FP16 maps + learned proposal against the plain FP32 search at equal median gap
+        from adock_b200 import synth
+        from adock_b200.proposal import ab_compare
+        rec2 = synth.config_receptor(2)
+        train = synth.ligand_set(args.screen_train, (8, 80), (0, 20), seed0=300_000)
+        held = synth.ligand_set(args.screen_eval, (8, 80), (0, 20), seed0=400_000)
+        t0 = time.perf_counter()
+        out["screening"] = ab_compare(rec2, train, held, device=dev, budgets=(250, 500, 1000, 2000),
+                                      learned=variants)
+        out["screening"]["wall_s"] = time.perf_counter() - t0
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = _cpu_baseline(ligs, rec, cfg)
     return out
@@ -401,11 +417,12 @@ def main():
         import datetime
         import torch
         import torch.distributed as dist
+        # the longest gap between two collectives is the warm-up (autotune + 3 steps, well under a minute)
         if args.impl == "ours":
             torch.cuda.set_device(local_rank)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
         else:
-            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=180))
     if args.impl == "reference":
         out = run_reference(args, rank, world)
     else:

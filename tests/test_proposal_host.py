@@ -62,3 +62,10 @@ def test_moves_to_identity_is_zero():
     target[:, 3] = 1.0
     y = moves_to(states, target)
     assert torch.all(y[:, :26] == 0) and torch.all(y[:, 26] == 5)
+
+
+def test_ligand_best_chain():
+    from adock_b200.proposal import ligand_best_chain
+    chain_lig = torch.tensor([0, 0, 0, 1, 1, 2, 2, 2], dtype=torch.int32)
+    best_e = torch.tensor([3.0, -1.0, 2.0, 5.0, 4.0, 1.0, 1.0, 7.0])
+    assert ligand_best_chain(chain_lig, best_e).tolist() == [1, 4, 6]
