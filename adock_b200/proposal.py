@@ -243,7 +243,7 @@ def _best_per_ligand(best_e, L, M):
 
 
 def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(125, 250, 500, 1000, 2000),
-               ref_steps=8000, train_steps=500, log_cap=2_000_000, epochs=3, learned=(("learned_f16", 32, 0.5),),
+               ref_steps=8000, train_steps=500, log_cap=2_000_000, epochs=3, learned=(("learned_f16", 32, 0.3),),
                seed=0, log=None):
     """Learned proposal vs plain MC at equal step budget (config-3 style evaluation).
 
@@ -352,7 +352,7 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
 
 
 def run_mc_segments(kp, net, chain_lig, chain_id, cur, cur_e, best, best_e, cfg, seed, prop_k=32, init_opt=True,
-                    stats=None, prop_frac=0.5):
+                    stats=None, prop_frac=0.3):
     """MC with learned proposals: the run is cut into segments of prop_k steps; before each segment the network
     reads every chain's current state and draws prop_k target states per chain around it (adock_prop_sample); a
     step proposes the next of them with probability prop_frac, else it takes the plain random move (and plain MC

@@ -49,7 +49,7 @@ def _args():
     ap.add_argument("--ab", action="store_true", help="learned proposal vs plain MC at equal step budget")
     ap.add_argument("--ab-train", type=int, default=256, help="fresh ligands for the proposal's training data")
     ap.add_argument("--ab-eval", type=int, default=256, help="held-out ligands for the A/B comparison")
-    ap.add_argument("--ab-variants", default="learned_f16:32:0.5",
+    ap.add_argument("--ab-variants", default="learned_f16:32:0.3",
                     help="learned variants name:segment_steps:learned_fraction[:chain|ligand training target], "
                          "comma separated")
     ap.add_argument("--screen", action="store_true",
