@@ -43,53 +43,65 @@ __global__ void prepare_kernel(adock_ligands_t lig, TypeTables tt, float4* atoms
     }
 }
 
-// Intra-pair schedule (one warp per ligand): the np pairs are placed into R = ceil(np / 32) rounds of 32 slots so
-// that each atom appears as few times as possible per round. Greedy in pair order: among the rounds with a free
-// slot, the one where the larger of the two atoms' current counts is smallest (then their sum, then the lowest
-// round). Empty slots get x = -1. The force atomics of one round in eval_eg then collide at most a few ways
-// (small ligands cannot avoid it: a round of 32 pairs needs 64 atom slots).
-__global__ void schedule_pairs_kernel(adock_ligands_t lig, TypeTables tt, int2* pairs, int P_pad) {
-    __shared__ unsigned char cnt[PAIR_ROUNDS_MAX][128];
-    __shared__ int fill[PAIR_ROUNDS_MAX];
+// Intra-pair schedule (one warp per ligand): the np pairs are placed into R = ceil(np / 32) rounds of 32 slots.
+// eval_eg adds a pair's force to its first atom with one set of shared-memory atomics and to its second atom with
+// another, so within a round only repeats of an atom on the same side collide (and serialise the atomic). The
+// Vina pair term is symmetric, so each pair may also be stored either way round. Greedy in pair order: over the
+// rounds with a free slot and both orientations, the choice where the larger of (the first atom's count as a first
+// atom, the second atom's count as a second atom) is smallest, then their sum, then the lowest round, then the
+// given orientation. Empty slots get x = -1. Counts live in dynamic shared memory, [R_cap][AM] per side; ligands
+// with more than R_cap rounds keep the pair order.
+__global__ void schedule_pairs_kernel(adock_ligands_t lig, TypeTables tt, int2* pairs, int P_pad, int R_cap) {
+    extern __shared__ int sched_smem[];
     const int l = blockIdx.x, lane = threadIdx.x;
     const int np = lig.np[l], AM = lig.AM, P = lig.P;
     const int R = (np + 31) / 32;
+    int* fill = sched_smem;                                            // [R_cap]
+    unsigned char* c1 = (unsigned char*)(sched_smem + R_cap);          // [R_cap][AM] count as first atom
+    unsigned char* c2 = c1 + (size_t)R_cap * AM;                       // [R_cap][AM] count as second atom
     int2* out = pairs + (long long)l * P_pad;
-    auto record = [&](int q) {
+    auto record = [&](int q, int swap) {
         const int i = lig.pr[((long long)l * P + q) * 2], j = lig.pr[((long long)l * P + q) * 2 + 1];
         int ti = lig.typ[(long long)l * AM + i], tj = lig.typ[(long long)l * AM + j];
         ti = ti < 0 ? 0 : (ti & 63);
         tj = tj < 0 ? 0 : (tj & 63);
         const int fl = hyd_pair(tt.flags[ti], tt.flags[tj]) | hb_pair(tt.flags[ti], tt.flags[tj]);
-        return make_int2((i & 0xff) | ((j & 0xff) << 8) | (fl << 16), __float_as_int(tt.radius[ti] + tt.radius[tj]));
+        const int a = swap ? j : i, b = swap ? i : j;
+        return make_int2((a & 0xff) | ((b & 0xff) << 8) | (fl << 16), __float_as_int(tt.radius[ti] + tt.radius[tj]));
     };
-    if (R > PAIR_ROUNDS_MAX) {  // very large ligands: keep the pair order
-        for (int q = lane; q < P_pad; q += 32) out[q] = q < np ? record(q) : make_int2(-1, 0);
+    if (R > R_cap) {  // very large ligands: keep the pair order
+        for (int q = lane; q < P_pad; q += 32) out[q] = q < np ? record(q, 0) : make_int2(-1, 0);
         return;
     }
-    for (int r = lane; r < PAIR_ROUNDS_MAX; r += 32) {
+    for (int r = lane; r < R; r += 32) {
         fill[r] = 0;
-        for (int a = 0; a < 128; ++a) cnt[r][a] = 0;
+        for (int a = 0; a < AM; ++a) {
+            c1[(size_t)r * AM + a] = 0;
+            c2[(size_t)r * AM + a] = 0;
+        }
     }
     __syncwarp();
     for (int q = 0; q < np; ++q) {
-        const int i = lig.pr[((long long)l * P + q) * 2] & 127, j = lig.pr[((long long)l * P + q) * 2 + 1] & 127;
+        const int i = lig.pr[((long long)l * P + q) * 2] % AM, j = lig.pr[((long long)l * P + q) * 2 + 1] % AM;
         unsigned best = 0xffffffffu;
         for (int r = lane; r < R; r += 32) {
             if (fill[r] < 32) {
-                const unsigned ci = cnt[r][i], cj = cnt[r][j];
-                const unsigned key = (((ci > cj ? ci : cj) * 64u + ci + cj) << 16) | (unsigned)r;
-                best = key < best ? key : best;
+#pragma unroll
+                for (int o = 0; o < 2; ++o) {
+                    const unsigned x = c1[(size_t)r * AM + (o ? j : i)], y = c2[(size_t)r * AM + (o ? i : j)];
+                    const unsigned key = (((x > y ? x : y) * 64u + x + y) << 17) | ((unsigned)r << 1) | (unsigned)o;
+                    best = key < best ? key : best;
+                }
             }
         }
         best = __reduce_min_sync(0xffffffffu, best);
-        const int found = (int)(best & 0xffffu);
+        const int found = (int)((best >> 1) & 0xffffu), o = (int)(best & 1u);
         if (lane == 0) {
             const int slot = found * 32 + fill[found];
             fill[found] += 1;
-            cnt[found][i] += 1;
-            cnt[found][j] += 1;
-            out[slot] = record(q);
+            c1[(size_t)found * AM + (o ? j : i)] += 1;
+            c2[(size_t)found * AM + (o ? i : j)] += 1;
+            out[slot] = record(q, o);
         }
         __syncwarp();
     }
@@ -292,7 +304,11 @@ extern "C" int adock_prepare(const adock_ligands_t* lig, const adock_sf_t* sf, a
     prepare_kernel<<<lig->L, 128, 0, st>>>(*lig, tt, (float4*)work->atoms, (uint32_t*)work->masks, (float4*)work->tors,
                                            (int4*)work->info, (float*)work->rg);
     ADOCK_CUDA(cudaGetLastError());
-    schedule_pairs_kernel<<<lig->L, 32, 0, st>>>(*lig, tt, (int2*)work->pairs, pad32(lig->P));
+    const int R_cap = min(pad32(lig->P) / 32, PAIR_ROUNDS_MAX);
+    const size_t sched_smem = (size_t)R_cap * sizeof(int) + 2 * (size_t)R_cap * lig->AM;
+    ADOCK_CUDA(cudaFuncSetAttribute(schedule_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sched_smem));
+    schedule_pairs_kernel<<<lig->L, 32, sched_smem, st>>>(*lig, tt, (int2*)work->pairs, pad32(lig->P), R_cap);
     ADOCK_CUDA(cudaGetLastError());
     return ADOCK_OK;
 }

@@ -250,7 +250,8 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
     1. Training data: plain FP32 search (Stage-A starts, ``train_steps`` MC steps) on ``train_ligs`` with the
        move log on; the network is trained on it (``epochs`` of Adam).
     2. Reference: plain FP32 search with ``ref_steps`` steps on the held-out ``eval_ligs``; E_ref(l) = the lowest
-       best energy over the ligand's chains (also over all runs below, so gaps are >= 0).
+       best energy over the ligand's chains (also over all runs below, so gaps are >= 0). The long run is also
+       reported as the plain FP32 search's row at ``ref_steps``.
     3. For each budget S: plain FP32, plain FP16 and each learned FP16 variant (name, segment length prop_k,
        learned fraction prop_frac; proposals with plain fallback) from the same Stage-A starts;
        gap(l) = E(l) - E_ref(l); reported: median and mean gap, ligands/s of Stage A + MC, evaluations per step.
@@ -312,7 +313,7 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
         st["evals_per_step"] = (int(kp.evals[0]) - ev0) / (cur.shape[0] * steps)
         return _best_per_ligand(be, L, chains), ev[0].elapsed_time(ev[1]), st
 
-    ref, ref_ms, _ = run("plain_f32", ref_steps)
+    ref, ref_ms, ref_st = run("plain_f32", ref_steps)
     results = {}
     out["learned_variants"] = {n: {"prop_k": k, "prop_frac": f, "target": t} for n, (k, f, t) in variants.items()}
     for m in ("plain_f32", "plain_f16", *variants):
@@ -322,14 +323,15 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
     for (e, _, _) in results.values():
         floor = torch.minimum(floor, e)
     out["reference"] = {"ms": ref_ms, "median_best": float(ref.median())}
+    results[("plain_f32", ref_steps)] = (ref, ref_ms, ref_st)   # the long run is also the plain search's last budget
     rows = {}
-    for (m, S), (e, ms, st) in results.items():
+    for (m, S), (e, ms, st) in sorted(results.items(), key=lambda kv: (kv[0][0], kv[0][1])):
         gap = (e - floor).cpu()
         rows.setdefault(m, []).append({"steps": S, "median_gap": float(gap.median()), "mean_gap": float(gap.mean()),
                                        "ligands_per_s": L / (ms / 1e3), "ms": ms, **st})
     out["methods"] = rows
     # equal-gap comparison: the budget each method needs to reach the plain FP32 median gap at its largest budget
-    target = rows["plain_f32"][-1]["median_gap"]
+    target = next(r["median_gap"] for r in rows["plain_f32"] if r["steps"] == max(budgets))
     out["target_gap"] = target
     for m, rs in rows.items():
         ok = [r for r in rs if r["median_gap"] <= target + 1e-6]

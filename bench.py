@@ -335,7 +335,7 @@ def run_ours(args, rank, world, local_rank):
         train = synth.ligand_set(args.screen_train, (8, 80), (0, 20), seed0=300_000)
         held = synth.ligand_set(args.screen_eval, (8, 80), (0, 20), seed0=400_000)
         t0 = time.perf_counter()
-        out["screening"] = ab_compare(rec2, train, held, device=dev, budgets=(250, 500, 1000, 2000),
+        out["screening"] = ab_compare(rec2, train, held, device=dev, budgets=(250, 500, 1000, 2000, 4000),
                                       learned=variants)
         out["screening"]["wall_s"] = time.perf_counter() - t0
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
