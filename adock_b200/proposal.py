@@ -206,6 +206,23 @@ def collect(kp, chain_lig, chain_id, cur, cur_e, best, best_e, cfg, seed, cap, i
     return lx[:n], (y_chain if target == "chain" else y_lig)
 
 
+def collect_learned(kp, net, chain_lig, chain_id, cur, cfg, seed, cap, prop_k=32, prop_frac=0.3):
+    """The learned search (``run_mc_segments`` with ``net``) from the states ``cur`` with the training-data log on;
+    returns (X, Y) as ``collect`` does, the targets being the learned search's own final minima of each chain."""
+    dev = kp.device
+    N = cur.shape[0]
+    best = cur.clone()
+    ce, be = torch.zeros(N, device=dev), torch.full((N,), float("inf"), device=dev)
+    lx = torch.empty(cap, IN, dtype=torch.bfloat16, device=dev)
+    ly = torch.empty(cap, 32, device=dev)
+    ln = torch.zeros(1, dtype=torch.int32, device=dev)
+    run_mc_segments(kp, net, chain_lig, chain_id, cur, ce, best, be, cfg, seed, prop_k=prop_k, prop_frac=prop_frac,
+                    log=(lx, ly, ln))
+    n = min(int(ln), cap)
+    states = ly[:n]
+    return lx[:n], moves_to(states, best[states[:, 28].long()])
+
+
 def _starts(prob, kp, cfg, seed):
     """Stage-A start poses of every chain (the search driver's first stage), packed as MC states."""
     from .search import stage_a_kernel
@@ -268,22 +285,35 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
     best = cur.clone()
     ce, be = torch.zeros(N, device=dev), torch.full((N,), float("inf"), device=dev)
     torch.cuda.synchronize(dev)
-    # learned variants: (name, segment steps, learned fraction[, training target "chain" | "ligand"])
+    # learned variants: (name, segment steps, learned fraction[, training "chain" | "ligand" | "dagger"]): the
+    # chain's or the ligand's best pose as target, or the chain network fine-tuned on its own search's moves
     variants = {v[0]: (v[1], v[2], v[3] if len(v) > 3 else "chain") for v in learned}
     X, Yc, Yl = collect(kp_t, cl, ci, cur, ce, best, be, cfg_tr, seed=seed + 1, cap=log_cap, target="both")
     nets = {}
     out["train"] = {"moves": int(X.shape[0]), "epochs": epochs}
-    for tgt in sorted({t for (_, _, t) in variants.values()}):
-        Y = Yc if tgt == "chain" else Yl
-        net = ProposalNet(dev, seed=seed)
+    targets = {t for (_, _, t) in variants.values()} | ({"chain"} if any(t == "dagger" for (_, _, t) in
+                                                                           variants.values()) else set())
+    for tgt in sorted(targets, key=lambda t: (t != "chain", t)):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        loss = net.fit(X, Y, epochs=epochs, batch=4096, lr=1e-3, seed=seed, log=log)
+        if tgt == "dagger":
+            # second round: the chain-target network drives the search on the training ligands with the log on;
+            # a copy fine-tuned on those moves (targets: the learned search's own final minima)
+            net = ProposalNet(dev, seed=seed)
+            net.load_state_dict(nets["chain"].state_dict())
+            cl2, ci2, cur2 = _starts(prob_t, kp_t, cfg_tr, seed + 5)
+            X2, Y2 = collect_learned(kp_t, nets["chain"], cl2, ci2, cur2, cfg_tr, seed + 6, log_cap)
+            loss = net.fit(X2, Y2, epochs=epochs, batch=4096, lr=5e-4, seed=seed + 1, log=log)
+            out["train"]["dagger_moves"] = int(X2.shape[0])
+            del X2, Y2
+        else:
+            Y = Yc if tgt == "chain" else Yl
+            net = ProposalNet(dev, seed=seed)
+            loss = net.fit(X, Y, epochs=epochs, batch=4096, lr=1e-3, seed=seed, log=log)
         e1.record()
         torch.cuda.synchronize(dev)
         nets[tgt] = net
-        out["train"][tgt] = {"final_loss": loss, "train_ms": e0.elapsed_time(e1),
-                             "loss_untrained": float(ProposalNet(dev, seed=seed).loss_grad(X[:65536], Y[:65536])[0])}
+        out["train"][tgt] = {"final_loss": loss, "train_ms": e0.elapsed_time(e1)}
     del X, Yc, Yl, kp_t, prob_t
     # 2./3. evaluation on held-out ligands
     probs = {"f32": _problem_for(rec, eval_ligs, dev, "f32")}
@@ -354,11 +384,12 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
 
 
 def run_mc_segments(kp, net, chain_lig, chain_id, cur, cur_e, best, best_e, cfg, seed, prop_k=32, init_opt=True,
-                    stats=None, prop_frac=0.3):
+                    stats=None, prop_frac=0.3, log=None):
     """MC with learned proposals: the run is cut into segments of prop_k steps; before each segment the network
     reads every chain's current state and draws prop_k target states per chain around it (adock_prop_sample); a
     step proposes the next of them with probability prop_frac, else it takes the plain random move (and plain MC
-    after 8 consecutive rejections of learned proposals)."""
+    after 8 consecutive rejections of learned proposals). log: the training-data log of run_mc, kept across the
+    segments."""
     steps = cfg["mc_steps"]
     pst = torch.zeros(4, dtype=torch.int64, device=kp.device)
     for sg in range(math.ceil(steps / prop_k)):
@@ -368,7 +399,7 @@ def run_mc_segments(kp, net, chain_lig, chain_id, cur, cur_e, best, best_e, cfg,
         moves = kp.prop_sample(chain_lig, chain_id, out, cur, k, seed ^ 0x5EEDBA5E, sg)
         kp.run_mc(chain_lig, chain_id, cur, cur_e, best, best_e, init_opt and sg == 0, k, cfg["bfgs_iters"],
                   cfg["mc_temperature"], cfg["mc_amp_pos"], cfg["mc_amp_rot"], seed, sg * prop_k, prop=moves,
-                  prop_stats=pst, prop_frac=prop_frac)
+                  prop_stats=pst, prop_frac=prop_frac, log=log)
     if stats is not None:
         p, pa, q, qa = pst.tolist()
         stats.update(prop_steps=p, prop_accepted=pa, plain_steps=q, plain_accepted=qa)

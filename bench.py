@@ -50,7 +50,7 @@ def _args():
     ap.add_argument("--ab-train", type=int, default=256, help="fresh ligands for the proposal's training data")
     ap.add_argument("--ab-eval", type=int, default=256, help="held-out ligands for the A/B comparison")
     ap.add_argument("--ab-variants", default="learned_f16:32:0.3",
-                    help="learned variants name:segment_steps:learned_fraction[:chain|ligand training target], "
+                    help="learned variants name:segment_steps:learned_fraction[:chain|ligand|dagger training], "
                          "comma separated")
     ap.add_argument("--screen", action="store_true",
                     help="screening comparison on the 8,000-atom receptor with 8-80-atom ligands (FP16 + learned "
@@ -130,15 +130,20 @@ def _peaks():
     return 6650.0, "fallback"
 
 
-def _traffic_per_atom_eval():
-    """DRAM bytes per atom evaluation of the MC kernel from the committed ncu summary (None if absent)."""
+def _profile_figure(name):
+    """A per-evaluation figure of the MC kernel from the committed ncu summary (None if absent):
+    dram_bytes_per_atom_eval, warp_instructions_per_eval."""
     f = ROOT / "profiles" / "mc_kernel_traffic.txt"
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
-        if line.startswith("dram_bytes_per_atom_eval:"):
+        if line.startswith(name + ":"):
             return float(line.split(":")[1])
     return None
+
+
+def _traffic_per_atom_eval():
+    return _profile_figure("dram_bytes_per_atom_eval")
 
 
 def run_reference(args, rank, world):
@@ -306,6 +311,15 @@ def run_ours(args, rank, world, local_rank):
             "peak_source": peak_kind, "kernel": "mc_kernel",
             "traffic": (tpa * atom_evals / args.steps) if tpa is not None else None,
             "algorithmic_bytes_per_launch": alg_bytes / args.steps, "launch_ms": 1e3 * mc_s / args.steps}
+    # the bound that applies to this gather/latency-bound kernel: warp-instruction issue (148 SMs x 4 schedulers x
+    # 1 instruction per clock at the SM clock seen during the run), with the instructions per evaluation from ncu
+    ipe = _profile_figure("warp_instructions_per_eval")
+    if ipe is not None and clk.get("sm_mhz"):
+        n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
+        issue_peak = n_sm * 4 * clk["sm_mhz"] * 1e6
+        issue = ipe * evals / mc_s
+        roof["issue"] = {"achieved": issue / 1e9, "peak": issue_peak / 1e9, "unit": "G warp-instr/s",
+                         "frac": issue / issue_peak, "instructions_per_eval": ipe}
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, shapes of the batched uneven workload)",

@@ -162,3 +162,9 @@ def test_features_log_training_and_proposal_mc(dev):
     torch.testing.assert_close(e_best, be, rtol=1e-4, atol=1e-4)
     assert stats["prop_steps"] + stats["plain_steps"] == M * cfg["mc_steps"]
     assert stats["prop_steps"] > 0
+    # a second round of training data from the learned search itself: moves logged across its segments
+    from adock_b200.proposal import collect_learned
+    X2, Y2 = collect_learned(kp, net, cl, ci, st.clone(), cfg, seed=11, cap=100000, prop_k=4)
+    assert X2.shape[0] > M and X2.shape[0] == Y2.shape[0]
+    Y2n = Y2.cpu().numpy()
+    assert np.isfinite(Y2n).all() and np.all(np.abs(Y2n[:, 6:26]) <= np.pi + 1e-4)
