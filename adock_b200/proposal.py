@@ -291,20 +291,29 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
     X, Yc, Yl = collect(kp_t, cl, ci, cur, ce, best, be, cfg_tr, seed=seed + 1, cap=log_cap, target="both")
     nets = {}
     out["train"] = {"moves": int(X.shape[0]), "epochs": epochs}
-    targets = {t for (_, _, t) in variants.values()} | ({"chain"} if any(t == "dagger" for (_, _, t) in
-                                                                           variants.values()) else set())
-    for tgt in sorted(targets, key=lambda t: (t != "chain", t)):
+    def rounds(t):   # "dagger" = 1 self-training round on top of "chain", "dagger2" = 2, ...
+        return int(t[6:] or 1) if t.startswith("dagger") else 0
+
+    def dagger_name(n):
+        return "chain" if n == 0 else ("dagger" if n == 1 else f"dagger{n}")
+
+    targets = {t for (_, _, t) in variants.values()}
+    for n in range(max(rounds(t) for t in targets)):
+        targets.add(dagger_name(n))
+    for tgt in sorted(targets, key=lambda t: (t == "ligand", rounds(t))):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        if tgt == "dagger":
-            # second round: the chain-target network drives the search on the training ligands with the log on;
-            # a copy fine-tuned on those moves (targets: the learned search's own final minima)
+        n = rounds(tgt)
+        if n > 0:
+            # self-training round n: the previous round's network drives the search on the training ligands with
+            # the log on; a copy of it is fine-tuned on those moves (targets: that search's own final minima)
+            prev = nets[dagger_name(n - 1)]
             net = ProposalNet(dev, seed=seed)
-            net.load_state_dict(nets["chain"].state_dict())
-            cl2, ci2, cur2 = _starts(prob_t, kp_t, cfg_tr, seed + 5)
-            X2, Y2 = collect_learned(kp_t, nets["chain"], cl2, ci2, cur2, cfg_tr, seed + 6, log_cap)
-            loss = net.fit(X2, Y2, epochs=epochs, batch=4096, lr=5e-4, seed=seed + 1, log=log)
-            out["train"]["dagger_moves"] = int(X2.shape[0])
+            net.load_state_dict(prev.state_dict())
+            cl2, ci2, cur2 = _starts(prob_t, kp_t, cfg_tr, seed + 5 * n)
+            X2, Y2 = collect_learned(kp_t, prev, cl2, ci2, cur2, cfg_tr, seed + 5 * n + 1, log_cap)
+            loss = net.fit(X2, Y2, epochs=epochs, batch=4096, lr=5e-4, seed=seed + n, log=log)
+            out["train"][f"{tgt}_moves"] = int(X2.shape[0])
             del X2, Y2
         else:
             Y = Yc if tgt == "chain" else Yl
@@ -380,7 +389,30 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
     for m in ("plain_f16", *variants):
         if b.get(m) and b.get("plain_f32"):
             out[f"speedup_at_gap_0.1_{m}"] = b[m]["ligands_per_s"] / b["plain_f32"]["ligands_per_s"]
+    # the same between budgets: steps to a 0.1 median gap by log-log interpolation of the gap between the two
+    # budgets that bracket it, ligands/s there by linear interpolation of the time per ligand
+    c = out["interp_at_gap_0.1"] = {m: interp_to_gap(rs, 0.1) for m, rs in rows.items()}
+    for m in ("plain_f16", *variants):
+        if c.get(m) and c.get("plain_f32"):
+            out[f"speedup_interp_at_gap_0.1_{m}"] = c[m]["ligands_per_s"] / c["plain_f32"]["ligands_per_s"]
     return out
+
+
+def interp_to_gap(rows, gap):
+    """Steps and ligands/s at which a method's median gap reaches ``gap``, interpolated between the two budgets
+    that bracket it (log gap linear in log steps; time per ligand linear in steps); None if no budget reaches it,
+    the first budget itself if it already does."""
+    rs = sorted(rows, key=lambda r: r["steps"])
+    for lo, hi in zip([None] + rs[:-1], rs):
+        if hi["median_gap"] <= gap:
+            if lo is None or lo["median_gap"] <= gap or hi["median_gap"] <= 0:
+                return {"steps": hi["steps"], "ligands_per_s": hi["ligands_per_s"]}
+            f = (math.log(gap) - math.log(lo["median_gap"])) / (math.log(hi["median_gap"]) - math.log(lo["median_gap"]))
+            s = math.exp(math.log(lo["steps"]) + f * (math.log(hi["steps"]) - math.log(lo["steps"])))
+            w = (s - lo["steps"]) / (hi["steps"] - lo["steps"])
+            t = (1 - w) / lo["ligands_per_s"] + w / hi["ligands_per_s"]
+            return {"steps": s, "ligands_per_s": 1.0 / t}
+    return None
 
 
 def run_mc_segments(kp, net, chain_lig, chain_id, cur, cur_e, best, best_e, cfg, seed, prop_k=32, init_opt=True,

@@ -57,6 +57,9 @@ def _args():
                          "proposal vs plain FP32 at equal median gap)")
     ap.add_argument("--screen-train", type=int, default=512, help="fresh ligands for the screening proposal's training")
     ap.add_argument("--screen-eval", type=int, default=1024, help="held-out ligands of the screening comparison")
+    ap.add_argument("--screen-variants", default="learned_f16:32:0.3:chain,learned_dagger:32:0.3:dagger",
+                    help="learned variants of the screening comparison (as --ab-variants; dagger, dagger2, ...: "
+                         "that many self-training rounds)")
     return ap.parse_args()
 
 
@@ -330,10 +333,14 @@ def run_ours(args, rank, world, local_rank):
            "mc_autotune": __import__("adock_b200.autotune", fromlist=["cached"]).cached()}
     if rank == 0 and world == 1 and not args.no_extras:
         out["grid_and_precision"] = _grid_and_precision(dev, ligs)
-    variants = []
-    for v in args.ab_variants.split(","):
-        f = v.split(":")
-        variants.append((f[0], int(f[1]), float(f[2])) + ((f[3],) if len(f) > 3 else ()))
+    def parse_variants(spec):
+        out_v = []
+        for v in spec.split(","):
+            f = v.split(":")
+            out_v.append((f[0], int(f[1]), float(f[2])) + ((f[3],) if len(f) > 3 else ()))
+        return out_v
+
+    variants = parse_variants(args.ab_variants)
     if rank == 0 and world == 1 and args.ab:
         from adock_b200 import synth
         from adock_b200.proposal import ab_compare
@@ -350,7 +357,7 @@ def run_ours(args, rank, world, local_rank):
         held = synth.ligand_set(args.screen_eval, (8, 80), (0, 20), seed0=400_000)
         t0 = time.perf_counter()
         out["screening"] = ab_compare(rec2, train, held, device=dev, budgets=(250, 500, 1000, 2000, 4000),
-                                      learned=variants)
+                                      learned=parse_variants(args.screen_variants))
         out["screening"]["wall_s"] = time.perf_counter() - t0
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = _cpu_baseline(ligs, rec, cfg)

@@ -69,3 +69,17 @@ def test_ligand_best_chain():
     chain_lig = torch.tensor([0, 0, 0, 1, 1, 2, 2, 2], dtype=torch.int32)
     best_e = torch.tensor([3.0, -1.0, 2.0, 5.0, 4.0, 1.0, 1.0, 7.0])
     assert ligand_best_chain(chain_lig, best_e).tolist() == [1, 4, 6]
+
+
+def test_interp_to_gap():
+    from adock_b200.proposal import interp_to_gap
+    rows = [{"steps": 500, "median_gap": 0.4, "ligands_per_s": 100.0},
+            {"steps": 1000, "median_gap": 0.05, "ligands_per_s": 50.0},
+            {"steps": 2000, "median_gap": 0.01, "ligands_per_s": 25.0}]
+    r = interp_to_gap(rows, 0.1)
+    # log-log: 0.4 -> 0.05 over a doubling is a factor 8 = 2^3; 0.1 is 2^2 below 0.4, so 2/3 of the doubling
+    assert abs(r["steps"] - 500 * 2 ** (2 / 3)) < 1e-6
+    w = (r["steps"] - 500) / 500
+    assert abs(1 / r["ligands_per_s"] - ((1 - w) / 100 + w / 50)) < 1e-12
+    assert interp_to_gap(rows, 0.5) == {"steps": 500, "ligands_per_s": 100.0}
+    assert interp_to_gap(rows, 0.001) is None
