@@ -10,7 +10,7 @@ Training data come from the plain search itself (``collect``): the MC kernel log
 lowered the chain's energy, the features of the pre-move state and the state; the target is the move from that
 state to the chain's best state at the end of the run. In the search (``run_mc_segments``) a fraction of the
 steps take the network's move instead of the random perturbation (the sampled spread has floors so the moves keep
-exploring); the Vina-form energy with BFGS and the Metropolis test still judge every move, and a chain whose
+exploring); the Vina-form energy with BFGS and the Metropolis test still decide every move, and a chain whose
 learned moves are rejected 8 times in a row falls back to plain MC until it accepts a move.
 """
 from __future__ import annotations

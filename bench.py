@@ -57,7 +57,7 @@ def _args():
                          "proposal vs plain FP32 at equal median gap)")
     ap.add_argument("--screen-train", type=int, default=512, help="fresh ligands for the screening proposal's training")
     ap.add_argument("--screen-eval", type=int, default=1024, help="held-out ligands of the screening comparison")
-    ap.add_argument("--screen-variants", default="learned_f16:32:0.3:chain,learned_dagger:32:0.3:dagger",
+    ap.add_argument("--screen-variants", default="learned_f16:32:0.3:chain,learned_dagger2:32:0.3:dagger2",
                     help="learned variants of the screening comparison (as --ab-variants; dagger, dagger2, ...: "
                          "that many self-training rounds)")
     return ap.parse_args()
