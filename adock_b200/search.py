@@ -175,10 +175,12 @@ def dock_problem_kernel(prob, boxes_c, boxes_s, cfg, seed=0, log=None, stats=Non
     chain_steps = 0
     seed64 = int(seed) * 1_000_003 + 12345
     mc = (cfg["mc_temperature"], cfg["mc_amp_pos"], cfg["mc_amp_rot"], seed64)
-    ev = None
+    ev = mc_counts0 = None
     if stats is not None and dev.type == "cuda":
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
         ev[0].record()
+        if hasattr(kp, "evals"):
+            mc_counts0 = kp.evals.clone()   # the autotuner's sample launches above also count
     if n_seg == 0:
         kp.run_mc(chain_lig, chain_id, cur, cur_e, best, best_e, True, 0, cfg["bfgs_iters"], *mc, 0)
     for sg in range(n_seg):
@@ -244,7 +246,7 @@ def dock_problem_kernel(prob, boxes_c, boxes_s, cfg, seed=0, log=None, stats=Non
             ev_ = kp.evals.tolist()
             stats["evals"], stats["atom_evals"] = int(ev_[0]), int(ev_[1])
         if mc_counts is not None:
-            mc_ = mc_counts.tolist()
+            mc_ = (mc_counts - mc_counts0).tolist()
             stats["mc_evals"], stats["mc_atom_evals"] = int(mc_[0]), int(mc_[1])
     return res
 
