@@ -57,6 +57,7 @@ def _args():
                          "proposal vs plain FP32 at equal median gap)")
     ap.add_argument("--screen-train", type=int, default=512, help="fresh ligands for the screening proposal's training")
     ap.add_argument("--screen-eval", type=int, default=1024, help="held-out ligands of the screening comparison")
+    ap.add_argument("--screen-log-cap", type=int, default=2_000_000, help="training moves kept per collection")
     ap.add_argument("--screen-variants", default="learned_f16:32:0.3:chain,learned_dagger2:32:0.3:dagger2",
                     help="learned variants of the screening comparison (as --ab-variants; dagger, dagger2, ...: "
                          "that many self-training rounds)")
@@ -357,7 +358,7 @@ def run_ours(args, rank, world, local_rank):
         held = synth.ligand_set(args.screen_eval, (8, 80), (0, 20), seed0=400_000)
         t0 = time.perf_counter()
         out["screening"] = ab_compare(rec2, train, held, device=dev, budgets=(250, 500, 1000, 2000, 4000),
-                                      learned=parse_variants(args.screen_variants))
+                                      learned=parse_variants(args.screen_variants), log_cap=args.screen_log_cap)
         out["screening"]["wall_s"] = time.perf_counter() - t0
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = _cpu_baseline(ligs, rec, cfg)
