@@ -55,10 +55,10 @@ def _args():
     ap.add_argument("--screen", action="store_true",
                     help="screening comparison on the 8,000-atom receptor with 8-80-atom ligands (FP16 + learned "
                          "proposal vs plain FP32 at equal median gap)")
-    ap.add_argument("--screen-train", type=int, default=512, help="fresh ligands for the screening proposal's training")
+    ap.add_argument("--screen-train", type=int, default=1536, help="fresh ligands for the screening proposal's training")
     ap.add_argument("--screen-eval", type=int, default=1024, help="held-out ligands of the screening comparison")
-    ap.add_argument("--screen-log-cap", type=int, default=2_000_000, help="training moves kept per collection")
-    ap.add_argument("--screen-variants", default="learned_f16:32:0.3:chain,learned_dagger2:32:0.3:dagger2",
+    ap.add_argument("--screen-log-cap", type=int, default=4_000_000, help="training moves kept per collection")
+    ap.add_argument("--screen-variants", default="learned_dagger2:32:0.3:dagger2",
                     help="learned variants of the screening comparison (as --ab-variants; dagger, dagger2, ...: "
                          "that many self-training rounds)")
     return ap.parse_args()
