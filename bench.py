@@ -156,12 +156,7 @@ def run_reference(args, rank, world):
         return None
     import torch
     from oracle import ref as R
-    from adock_b200 import params
-    from adock_b200.grid import GridSet, grid_dims
-    from adock_b200.ligand import LigandBatch
-    from adock_b200.problem import PairPotential, Problem, pad_receptors
     from adock_b200.search import dock_problem_kernel
-    import numpy as np
     if not R.available():
         return {"impl": "reference", "unavailable": "oracle/_ref (the reference's CPU build) was not built on this tree"}
     threads = R.threads()
