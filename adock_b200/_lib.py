@@ -49,7 +49,7 @@ class McArgs(ctypes.Structure):
                 ("bfgs_iters", I), ("temp", F), ("amp_pos", F), ("amp_rot", F), ("seed", ctypes.c_ulonglong),
                 ("step_offset", I), ("exact", I), ("order", P), ("queue", P), ("evals", P), ("variant", I),
                 ("prop", P), ("prop_k", I), ("prop_stats", P), ("log_x", P), ("log_y", P), ("log_n", P),
-                ("log_cap", I), ("prop_frac", F)]
+                ("log_cap", I), ("prop_frac", F), ("lig_active", P)]
 
 
 SP = ctypes.POINTER
@@ -64,6 +64,13 @@ _SIGS = {
     "adock_mc": ([SP(Ligands), SP(Work), SP(Grids), SP(SF), SP(Receptors), SP(McArgs), P], I),
     "adock_stage_a": ([SP(Ligands), SP(Work), SP(Grids), SP(SF), P, I, P, I, P, P, I, F, P, P, P], I),
     "adock_neighbours": ([SP(Ligands), SP(Work), SP(SF), SP(Receptors), P, I, P, F, P, P, I, P], I),
+    "adock_stage_a_boxes": ([SP(Ligands), SP(Work), SP(Grids), SP(SF), P, I, P, I, P, P, I, P, F, P, P, P], I),
+    "adock_conformers": ([SP(Ligands), SP(Work), SP(SF), I, I, ctypes.c_ulonglong, P, P, P, P], I),
+    "adock_lattice": ([SP(Grids), I, P, P, P, P, F, F, I, P, P, P], I),
+    "adock_select_starts": ([I, I, I, I, I, P, P, P, P, P, P, P, I, P, P, P], I),
+    "adock_segment_update": ([I, I, I, I, I, F, P, P, P, P, P, P, P], I),
+    "adock_cluster": ([SP(Work), I, I, P, P, I, F, I, P, P, P], I),
+    "adock_pose_atoms": ([SP(Work), I, P, P, I, P, I, P, P, P], I),
     "adock_rescore64": ([SP(Ligands), SP(Work), SP(Grids), SP(SF), SP(Receptors), P, I, P, P, P, P, P], I),
     "adock_mc_noalloc_scratch_bytes": ([I, I, I, I], ctypes.c_size_t),
     "adock_mc_noalloc": ([SP(Ligands), SP(Grids), SP(SF), SP(Receptors), SP(McArgs), P], I),

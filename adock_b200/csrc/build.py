@@ -12,7 +12,8 @@ HERE = Path(__file__).resolve().parent
 PKG = HERE.parent
 ROOT = PKG.parent
 LIB = PKG / "libadock_b200.so"
-SOURCES = ["abi.cu", "grid.cu", "search.cu", "search_f32.cu", "search_f16.cu", "search_bf16.cu", "mlp.cu"]
+SOURCES = ["abi.cu", "grid.cu", "search.cu", "search_f32.cu", "search_f16.cu", "search_bf16.cu", "pipeline.cu",
+           "mlp.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-Xcompiler", "-fPIC",
          "-I", str(ROOT / "include")]

@@ -254,6 +254,12 @@ __global__ void __launch_bounds__(128) gemm_bf16_tc_kernel(const __grid_constant
         }
         __syncthreads();
         ok = fail_sh == 0;
+        if (!ok) {
+            // gave up waiting: before the tensor memory is released below, wait once more (bounded) for the MMAs
+            // of this stage that may still be running; the tile is not written (its contents are undefined)
+            tc_wait(mbar_a, (uint32_t)(kt & 1));
+            __syncthreads();
+        }
     }
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (ok && nk > 0) {

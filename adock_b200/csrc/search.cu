@@ -244,7 +244,7 @@ __global__ void prop_sample_kernel(const int4* info, const int* chain_lig, const
 }
 
 // ------------------------------------------------------------------------------------------ host side
-static TypeTables make_tables(const adock_sf_t* sf) {
+TypeTables make_tables(const adock_sf_t* sf) {
     TypeTables t;
     for (int i = 0; i < 64; ++i) {
         t.radius[i] = i < sf->n_types ? sf->radius[i] : 0.f;
@@ -253,7 +253,7 @@ static TypeTables make_tables(const adock_sf_t* sf) {
     return t;
 }
 
-static int make_params(SearchParams& P, const adock_ligands_t* lig, const adock_work_t* work, const adock_grids_t* grids,
+int make_params(SearchParams& P, const adock_ligands_t* lig, const adock_work_t* work, const adock_grids_t* grids,
                        const adock_sf_t* sf, const adock_receptors_t* rec) {
     ADOCK_CHECK_ARG(lig && work && sf, "null ligand/work/sf argument");
     ADOCK_CHECK_ARG(lig->AM % 32 == 0 && lig->AM >= 32 && lig->AM <= 128, "AM must be 32, 64, 96 or 128 (got %d)", lig->AM);
@@ -361,6 +361,7 @@ extern "C" int adock_mc(const adock_ligands_t* lig, const adock_work_t* work, co
     M.prop = mc->prop; M.prop_k = mc->prop_k; M.prop_stats = mc->prop_stats;
     M.prop_frac = (mc->prop_frac <= 0.f || mc->prop_frac >= 1.f) ? 1.f : mc->prop_frac;
     M.log_x = (__nv_bfloat16*)mc->log_x; M.log_y = mc->log_y; M.log_n = mc->log_n; M.log_cap = mc->log_cap;
+    M.lig_active = mc->lig_active;
     const TypeTables tt = make_tables(sf);
     cudaStream_t st = (cudaStream_t)stream;
     switch (grids->dtype) {
@@ -371,10 +372,10 @@ extern "C" int adock_mc(const adock_ligands_t* lig, const adock_work_t* work, co
     ADOCK_CHECK_ARG(false, "unknown grid dtype %d", grids->dtype);
 }
 
-extern "C" int adock_stage_a(const adock_ligands_t* lig, const adock_work_t* work, const adock_grids_t* grids,
-                             const adock_sf_t* sf, const float* conf, int C, const float* quats, int Q,
-                             const float* trans, const int* ntrans, int nt_max, float cap, float* best_e, int* best_i,
-                             void* stream) {
+static int stage_a_common(const adock_ligands_t* lig, const adock_work_t* work, const adock_grids_t* grids,
+                          const adock_sf_t* sf, const float* conf, int C, const float* quats, int Q, const float* trans,
+                          const int* ntrans, int nt_max, const int* lig_box, float cap, float* best_e, int* best_i,
+                          void* stream) {
     SearchParams P;
     int rc = make_params(P, lig, work, grids, sf, nullptr);
     if (rc) return rc;
@@ -386,14 +387,33 @@ extern "C" int adock_stage_a(const adock_ligands_t* lig, const adock_work_t* wor
     cudaStream_t st = (cudaStream_t)stream;
     switch (grids->dtype) {
         case ADOCK_GRID_F32:
-            return launch_stage_a<float>(P, blocks, conf, C, quats, Q, trans, ntrans, nt_max, cap, best_e, best_i, st);
+            return launch_stage_a<float>(P, blocks, conf, C, quats, Q, trans, ntrans, nt_max, lig_box, cap, best_e,
+                                         best_i, st);
         case ADOCK_GRID_F16:
-            return launch_stage_a<__half>(P, blocks, conf, C, quats, Q, trans, ntrans, nt_max, cap, best_e, best_i, st);
+            return launch_stage_a<__half>(P, blocks, conf, C, quats, Q, trans, ntrans, nt_max, lig_box, cap, best_e,
+                                          best_i, st);
         case ADOCK_GRID_BF16:
-            return launch_stage_a<__nv_bfloat16>(P, blocks, conf, C, quats, Q, trans, ntrans, nt_max, cap, best_e,
-                                                 best_i, st);
+            return launch_stage_a<__nv_bfloat16>(P, blocks, conf, C, quats, Q, trans, ntrans, nt_max, lig_box, cap,
+                                                 best_e, best_i, st);
     }
     ADOCK_CHECK_ARG(false, "unknown grid dtype %d", grids->dtype);
+}
+
+extern "C" int adock_stage_a(const adock_ligands_t* lig, const adock_work_t* work, const adock_grids_t* grids,
+                             const adock_sf_t* sf, const float* conf, int C, const float* quats, int Q,
+                             const float* trans, const int* ntrans, int nt_max, float cap, float* best_e, int* best_i,
+                             void* stream) {
+    return stage_a_common(lig, work, grids, sf, conf, C, quats, Q, trans, ntrans, nt_max, nullptr, cap, best_e, best_i,
+                          stream);
+}
+
+extern "C" int adock_stage_a_boxes(const adock_ligands_t* lig, const adock_work_t* work, const adock_grids_t* grids,
+                                   const adock_sf_t* sf, const float* conf, int C, const float* quats, int Q,
+                                   const float* trans, const int* ntrans, int nt_max, const int* lig_box, float cap,
+                                   float* best_e, int* best_i, void* stream) {
+    ADOCK_CHECK_ARG(lig_box, "null lig_box");
+    return stage_a_common(lig, work, grids, sf, conf, C, quats, Q, trans, ntrans, nt_max, lig_box, cap, best_e, best_i,
+                          stream);
 }
 
 extern "C" int adock_neighbours(const adock_ligands_t* lig, const adock_work_t* work, const adock_sf_t* sf,

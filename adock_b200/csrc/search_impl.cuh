@@ -88,6 +88,7 @@ struct McParams {
     float* log_y;
     int* log_n;
     int log_cap;
+    const int* lig_active;           // [L] or NULL: chains of a ligand with flag 0 are left unchanged
 };
 
 #define PROP_IN 288
@@ -680,6 +681,7 @@ __global__ void __launch_bounds__(128, MINB) mc_kernel(const __grid_constant__ S
         if (idx >= M.n_chains) break;
         const int ch = M.order ? M.order[idx] : idx;
         const int l = M.chain_lig[ch];
+        if (M.lig_active && M.lig_active[l] == 0) continue;
         const int cid = M.chain_id[ch];
         const unsigned n_eval_start = n_eval;
         Chain<APL> c;
@@ -813,8 +815,8 @@ __global__ void __launch_bounds__(128) eg_kernel(const __grid_constant__ SearchP
 template <typename GT>
 __global__ void __launch_bounds__(256) stage_a_kernel(const __grid_constant__ SearchParams P, const float* conf, int C,
                                                       const float* quats, int Q, const float* trans,
-                                                      const int* ntrans, int NT_MAX, float cap, float* best_e,
-                                                      int* best_i) {
+                                                      const int* ntrans, int NT_MAX, const int* lig_box,
+                                                      float cap, float* best_e, int* best_i) {
     extern __shared__ float4 smem4[];
     float4* X = smem4;  // [AM] rotated conformer + slot bits
     __shared__ float red_e[256];
@@ -847,9 +849,10 @@ __global__ void __launch_bounds__(256) stage_a_kernel(const __grid_constant__ Se
     const float inv = P.inv_s, pen = P.pen;
     float be = 3.4e38f;
     int bi = 0;
-    const int nT = ntrans[l];
+    const int box = lig_box ? lig_box[l] : l;   // translations per ligand, or per box shared by ligands
+    const int nT = ntrans[box];
     for (int ti = threadIdx.x; ti < nT; ti += blockDim.x) {
-        const float* T = trans + ((long long)l * NT_MAX + ti) * 3;
+        const float* T = trans + ((long long)box * NT_MAX + ti) * 3;
         const float T0 = T[0], T1 = T[1], T2 = T[2];
         float e = 0.f;
         for (int a = 0; a < n_at; ++a) {
@@ -1094,11 +1097,11 @@ int launch_eg(const SearchParams& P, const int* cl, int n, const float* state, f
 
 template <typename GT>
 int launch_stage_a(const SearchParams& P, long long blocks, const float* conf, int C, const float* quats, int Q,
-                   const float* trans, const int* ntrans, int nt_max, float cap, float* best_e, int* best_i,
-                   cudaStream_t st) {
+                   const float* trans, const int* ntrans, int nt_max, const int* lig_box, float cap, float* best_e,
+                   int* best_i, cudaStream_t st) {
     const size_t smem = (size_t)P.AM * sizeof(float4);
-    stage_a_kernel<GT><<<(unsigned)blocks, 256, smem, st>>>(P, conf, C, quats, Q, trans, ntrans, nt_max, cap, best_e,
-                                                            best_i);
+    stage_a_kernel<GT><<<(unsigned)blocks, 256, smem, st>>>(P, conf, C, quats, Q, trans, ntrans, nt_max, lig_box, cap,
+                                                            best_e, best_i);
     ADOCK_CUDA(cudaGetLastError());
     return ADOCK_OK;
 }
@@ -1129,7 +1132,8 @@ int launch_prop_features(const SearchParams& P, const int* cl, int n, const floa
     template int launch_eg<GT>(const SearchParams&, const int*, int, const float*, float*, float*, int,           \
                                const TypeTables&, cudaStream_t);                                                  \
     template int launch_stage_a<GT>(const SearchParams&, long long, const float*, int, const float*, int,         \
-                                    const float*, const int*, int, float, float*, int*, cudaStream_t);           \
+                                    const float*, const int*, int, const int*, float, float*, int*,              \
+                                    cudaStream_t);                                                                \
     template int launch_rescore64<GT>(const SearchParams&, const int*, int, const float*, double*, double*,       \
                                       float*, const TypeTables&, const adock_sf_t&, cudaStream_t);
 
@@ -1140,8 +1144,14 @@ int launch_prop_features(const SearchParams& P, const int* cl, int n, const floa
     extern template int launch_eg<GT>(const SearchParams&, const int*, int, const float*, float*, float*, int,    \
                                       const TypeTables&, cudaStream_t);                                           \
     extern template int launch_stage_a<GT>(const SearchParams&, long long, const float*, int, const float*, int,  \
-                                           const float*, const int*, int, float, float*, int*, cudaStream_t);    \
+                                           const float*, const int*, int, const int*, float, float*, int*,       \
+                                           cudaStream_t);                                                         \
     extern template int launch_rescore64<GT>(const SearchParams&, const int*, int, const float*, double*,         \
                                              double*, float*, const TypeTables&, const adock_sf_t&, cudaStream_t);
+
+// host helpers shared by the translation units of the search (defined in search.cu)
+TypeTables make_tables(const adock_sf_t* sf);
+int make_params(SearchParams& P, const adock_ligands_t* lig, const adock_work_t* work, const adock_grids_t* grids,
+                const adock_sf_t* sf, const adock_receptors_t* rec);
 
 }  // namespace adock

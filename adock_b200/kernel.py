@@ -169,13 +169,14 @@ class B200KernelProblem:
 
     def run_mc(self, chain_lig, chain_id, cur, cur_e, best, best_e, init_opt, mc_steps, bfgs_iters, temp,
                amp_pos, amp_rot, seed, step_offset, exact=False, nbr=None, nbr_n=None, order=None, variant=None,
-               prop=None, prop_stats=None, log=None, prop_frac=1.0):
+               prop=None, prop_stats=None, log=None, prop_frac=1.0, lig_active=None):
         """In place on cur/cur_e/best/best_e (float32 contiguous CUDA tensors). exact=True with nbr [N, NB] int32 /
         nbr_n [N]: each chain's exact inter energy loops only over its receptor-atom neighbour list.
         variant: MC launch variant (default: the tuned one, else the library default).
         prop: learned moves [N, k, 32] for steps 0..k-1 of this launch (plain MC fallback after 8 rejections);
         prop_stats: int64 [4] counters; log: (x BF16 [cap, 288], y [cap, 32], n int32 [1]) training-data log;
-        prop_frac: fraction of steps that take the learned move (the others take the plain random move)."""
+        prop_frac: fraction of steps that take the learned move (the others take the plain random move);
+        lig_active: int32 [L] device flags, chains of ligands with 0 are left unchanged (None: all run)."""
         N = cur.shape[0]
         if N == 0:
             return
@@ -213,6 +214,10 @@ class B200KernelProblem:
         if log is not None:
             lx, ly, ln = log
             a.log_x, a.log_y, a.log_n, a.log_cap = _lib.ptr(lx), _lib.ptr(ly), _lib.ptr(ln), int(lx.shape[0])
+        if lig_active is not None:
+            assert lig_active.dtype == torch.int32 and lig_active.is_contiguous() and lig_active.numel() == self.L
+            a.lig_active = _lib.ptr(lig_active)
+            keep.append(lig_active)
         with torch.cuda.device(self.device):
             _lib.call("adock_mc", self.c_lig, self.c_work, self.c_grids, self.c_sf, self.c_rec, a, _lib.stream_ptr())
         self._keep_mc = keep
@@ -231,6 +236,86 @@ class B200KernelProblem:
                       _lib.ptr(keep[1]), Q, _lib.ptr(keep[2]), _lib.ptr(keep[3]), NT, float(cap), _lib.ptr(be),
                       _lib.ptr(bi), _lib.stream_ptr())
         return be.view(L, C * Q), bi.view(L, C * Q).long()
+
+    # ---- device pipeline of the search driver (adock_b200.search) ----
+    def conformers(self, NT, C, seed):
+        """Stage-A conformers: (theta [L, C, KM], heavy-atom coordinates [L, C, AM, 3], intra energies [L, C])."""
+        L = self.L
+        theta = torch.empty(L, C, self.KM, device=self.device)
+        conf = torch.empty(L, C, self.AM, 3, device=self.device)
+        e = torch.empty(L, C, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.call("adock_conformers", self.c_lig, self.c_work, self.c_sf, int(NT), int(C),
+                      int(seed) & 0xFFFFFFFFFFFFFFFF, _lib.ptr(theta), _lib.ptr(conf), _lib.ptr(e), _lib.stream_ptr())
+        return theta, conf, e
+
+    def lattice(self, B, box, box_rec, box_slot, box_n, step, probe_max, nt_max):
+        """Probe-filtered translation lattices of B boxes: (trans [B, nt_max, 3], counts [B] int32)."""
+        trans = torch.empty(B, nt_max, 3, device=self.device)
+        cnt = torch.empty(B, dtype=torch.int32, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.call("adock_lattice", self.c_grids, int(B), _lib.ptr(box), _lib.ptr(box_rec), _lib.ptr(box_slot),
+                      _lib.ptr(box_n), float(step), float(probe_max), int(nt_max), _lib.ptr(trans), _lib.ptr(cnt),
+                      _lib.stream_ptr())
+        return trans, cnt
+
+    def stage_a_boxes(self, conf, quats, trans, ntrans, lig_box, cap):
+        """Rigid Stage-A scores with per-box lattices: (best_e [L, C*Q], best_i [L, C*Q] int32)."""
+        L, C = conf.shape[:2]
+        Q = quats.shape[0]
+        be = torch.empty(L, C * Q, device=self.device)
+        bi = torch.empty(L, C * Q, dtype=torch.int32, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.call("adock_stage_a_boxes", self.c_lig, self.c_work, self.c_grids, self.c_sf, _lib.ptr(conf), int(C),
+                      _lib.ptr(quats), int(Q), _lib.ptr(trans), _lib.ptr(ntrans), int(trans.shape[1]),
+                      _lib.ptr(lig_box), float(cap), _lib.ptr(be), _lib.ptr(bi), _lib.stream_ptr())
+        return be, bi
+
+    def select_starts(self, best_e, best_i, e_conf, quats, theta, trans, lig_box, M):
+        """M start states per ligand (state [L*M, SD], Stage-A energies [L*M])."""
+        L, C = e_conf.shape
+        Q = quats.shape[0]
+        state = torch.zeros(L * M, self.SD, device=self.device)
+        e = torch.empty(L * M, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.call("adock_select_starts", L, int(C), int(Q), self.KM, int(M), _lib.ptr(best_e), _lib.ptr(best_i),
+                      _lib.ptr(e_conf), _lib.ptr(quats), _lib.ptr(theta), _lib.ptr(trans), _lib.ptr(lig_box),
+                      int(trans.shape[1]), _lib.ptr(state), _lib.ptr(e), _lib.stream_ptr())
+        return state, e
+
+    def segment_update(self, L, M, seg, next_sg, es_rounds, es_tol, best_e, seg_lim, glob, stall, active,
+                       chain_steps):
+        """Per-ligand budget and early-stop flags after an MC segment (in place on glob, stall, active)."""
+        with torch.cuda.device(self.device):
+            _lib.call("adock_segment_update", int(L), int(M), int(seg), int(next_sg), int(es_rounds), float(es_tol),
+                      _lib.ptr(best_e), _lib.ptr(seg_lim), _lib.ptr(glob), _lib.ptr(stall), _lib.ptr(active),
+                      _lib.ptr(chain_steps), _lib.stream_ptr())
+
+    def cluster(self, e_total, X, L, P, cut, n_out):
+        """Greedy cluster representatives of P poses per ligand: (reps [L, n_out] int32, counts [L] int32)."""
+        reps = torch.empty(L, n_out, dtype=torch.int32, device=self.device)
+        cnt = torch.empty(L, dtype=torch.int32, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.call("adock_cluster", self.c_work, int(L), int(P), _lib.ptr(e_total.contiguous()),
+                      _lib.ptr(X.contiguous()), int(X.shape[1]), float(cut), int(n_out), _lib.ptr(reps), _lib.ptr(cnt),
+                      _lib.stream_ptr())
+        return reps, cnt
+
+    def pose_atoms(self, lb, chain_lig, states):
+        """All-atom world coordinates [n, A, 3] of states (atom order and padding of the LigandBatch lb)."""
+        if not hasattr(self, "_atoms_all") or self._atoms_all[0] is not lb:
+            ref = lb.ref.to(self.device, torch.float32).contiguous()
+            bits = torch.as_tensor(lb.atom_masks().view(np.int32), device=self.device).contiguous()
+            self._atoms_all = (lb, ref, bits)
+        _, ref, bits = self._atoms_all
+        n = states.shape[0]
+        X = torch.empty(n, lb.A, 3, device=self.device)
+        cl = self._i32(chain_lig)
+        st = states.to(self.device, torch.float32).contiguous()
+        with torch.cuda.device(self.device):
+            _lib.call("adock_pose_atoms", self.c_work, self.KM, _lib.ptr(ref), _lib.ptr(bits), int(lb.A), _lib.ptr(cl),
+                      int(n), _lib.ptr(st), _lib.ptr(X), _lib.stream_ptr())
+        return X
 
     def receptor_neighbours(self, prob, chain_lig, states, K, margin):
         """Per chain: indices of receptor atoms within cutoff + margin of any heavy atom of the chain's pose,

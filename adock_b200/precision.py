@@ -14,7 +14,7 @@ import torch
 from . import params
 from .grid import make_gridset
 from .kernel import B200KernelProblem
-from .ligand import LigandBatch, random_quat
+from .ligand import LigandBatch
 from .problem import PairPotential, Problem, pad_receptors
 
 
@@ -26,7 +26,8 @@ def random_poses(prob, kp, n_poses, seed=0, sigma=1.5):
     cl = (torch.arange(n_poses, device=dev) % L).to(torch.int32)
     c = (prob.gs.lo[0] + prob.gs.hi[0]) / 2
     t = c + torch.randn((n_poses, 3), generator=g, device=dev) * sigma
-    q = random_quat((n_poses,), g, dev)
+    q = torch.randn((n_poses, 4), generator=g, device=dev)
+    q = q / q.norm(dim=1, keepdim=True)                 # uniform on the unit 3-sphere
     th = (torch.rand((n_poses, prob.lb.K), generator=g, device=dev) * 2 - 1) * np.pi
     th = th * prob.lb.tvalid[cl.long()]
     return cl, kp.pack(t, q, th)

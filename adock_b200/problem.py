@@ -1,201 +1,163 @@
-"""Docking problem container and the host packing of a ligand batch for the search kernels.
+"""Docking problems and their packing into the search kernels' arrays.
 
-``Problem`` mirrors ``src/adock/search.py:65-132`` (grid set, ligand batch, receptor index per ligand, pair
-potential, optional receptor atoms for exact energies). ``pack_host`` restates ``src/adock/mckernel.py:547-599``:
-heavy atoms only, AM = 64 if the largest ligand has <= 64 heavy atoms else a multiple of 32, KM = a multiple
-of 8 >= the largest torsion count, P = the largest pair count.
+``Problem(gridset, lb, rec_idx, pot, rec=None)`` is the reference container (``src/adock/search.py:65-72``): maps,
+ligand batch, receptor of each ligand, pair potential and, for exact energies, the padded receptor atoms
+``(xyz [R, N, 3], types [R, N], mask [R, N])`` of ``pad_receptors`` (``search.py:369-379``).
+
+``pack_host`` produces the kernel input layout of the reference ``mckernel.pack_host`` (``mckernel.py:547-599``):
+heavy atoms only, AM = 64 when the largest ligand has <= 64 heavy atoms else a multiple of 32, KM = a multiple of
+8 >= the largest torsion count, P = the largest pair count; every array is one scatter over the concatenated
+ligands, with atom indices renumbered to heavy-atom order.
+
+``PairPotential`` carries the Vina-family parameters; its ``terms``/``energy`` evaluate the published pair terms
+(``scoring.py:18-31``) in torch, which the tests use as a float64 check of the kernels' constants.
 """
 from __future__ import annotations
-
-import math
 
 import numpy as np
 import torch
 
-from .ligand import internal_coords, pose_coords
+_PRM_KEYS = ("g1_off", "g1_w", "g2_off", "g2_w", "rep_off", "hyd_good", "hyd_bad", "hb_good", "hb_bad", "cutoff")
+_W_KEYS = ("w_g1", "w_g2", "w_rep", "w_hyd", "w_hb")
 
 
-class PairPotential:
-    """Vina-family pair potential (``src/adock/scoring.py:34-61``): ``p`` holds the flat parameters."""
-
-    def __init__(self, sfp, device="cpu"):
-        self.p = sfp
-        self.radius = torch.tensor(sfp["radius"], device=device)
-        self.hyd = torch.tensor(sfp["hydrophobic"], device=device).bool()
-        self.don = torch.tensor(sfp["donor"], device=device).bool()
-        self.acc = torch.tensor(sfp["acceptor"], device=device).bool()
-
-    def prm(self):
-        p = self.p
-        return (p["g1_off"], p["g1_w"], p["g2_off"], p["g2_w"], p["rep_off"], p["hyd_good"], p["hyd_bad"],
-                p["hb_good"], p["hb_bad"], p["cutoff"])
-
-    def weights(self, device=None):
-        p = self.p
-        return torch.tensor([p["w_g1"], p["w_g2"], p["w_rep"], p["w_hyd"], p["w_hb"]],
-                            device=device or self.radius.device)
-
-    def terms(self, r, ti, tj):
-        return pair_terms(r, ti, tj, self.radius, self.hyd, self.don, self.acc, self.prm())
-
-    def energy(self, r, ti, tj):
-        return (self.terms(r, ti, tj) * self.weights(r.device).to(r.dtype)).sum(-1)
-
-
-def _slope_step(x, good, bad):
-    if bad < good:
-        return torch.clamp((x - bad) / (good - bad), 0.0, 1.0)
-    return torch.clamp((bad - x) / (bad - good), 0.0, 1.0)
+def _ramp(d, good, bad):
+    """1 at d <= good, 0 at d >= bad, linear between (either orientation of good/bad)."""
+    return ((bad - d) / (bad - good)).clamp(0.0, 1.0)
 
 
 def pair_terms(r, ti, tj, radius, hyd, don, acc, prm):
-    """Unweighted Vina-family terms [..., 5] (``scoring.py:18-31``)."""
-    g1_off, g1_w, g2_off, g2_w, rep_off, hyd_good, hyd_bad, hb_good, hb_bad, cutoff = prm
-    radius = radius.to(r.dtype)
-    d = r - radius[ti] - radius[tj]
-    g1 = torch.exp(-((d - g1_off) / g1_w) ** 2)
-    g2 = torch.exp(-((d - g2_off) / g2_w) ** 2)
-    dr = d - rep_off
-    rep = torch.where(dr < 0, dr * dr, torch.zeros_like(dr))
-    hy = torch.where(hyd[ti] & hyd[tj], _slope_step(d, hyd_good, hyd_bad), torch.zeros_like(d))
-    hb = torch.where((don[ti] & acc[tj]) | (acc[ti] & don[tj]), _slope_step(d, hb_good, hb_bad), torch.zeros_like(d))
-    out = torch.stack([g1, g2, rep, hy, hb], -1)
-    return torch.where((r < cutoff).unsqueeze(-1), out, torch.zeros_like(out))
+    """Unweighted Vina-family terms [..., 5] = gauss1, gauss2, repulsion, hydrophobic, H-bond of pairs at distance
+    r with types ti, tj; zero at r >= cutoff. The surface distance is d = r - R_i - R_j."""
+    p = dict(zip(_PRM_KEYS, prm))
+    d = r - radius.to(r.dtype)[ti] - radius.to(r.dtype)[tj]
+    gauss = lambda off, w: torch.exp(-torch.square((d - off) / w))
+    rep = torch.square(torch.clamp(d - p["rep_off"], max=0.0))
+    hyd_pair = hyd[ti] & hyd[tj]
+    hb_pair = (don[ti] & acc[tj]) | (acc[ti] & don[tj])
+    zero = torch.zeros_like(d)
+    terms = torch.stack([gauss(p["g1_off"], p["g1_w"]), gauss(p["g2_off"], p["g2_w"]), rep,
+                         torch.where(hyd_pair, _ramp(d, p["hyd_good"], p["hyd_bad"]), zero),
+                         torch.where(hb_pair, _ramp(d, p["hb_good"], p["hb_bad"]), zero)], -1)
+    return terms * (r < p["cutoff"]).unsqueeze(-1).to(terms.dtype)
+
+
+class PairPotential:
+    """Vina-family pair potential (reference interface ``scoring.py:34-61``); ``p`` holds the flat parameters
+    (``params.sf_params``)."""
+
+    def __init__(self, sfp, device="cpu"):
+        self.p = sfp
+        self.radius = torch.tensor(np.asarray(sfp["radius"], np.float32), device=device)
+        self.hyd = torch.tensor(np.asarray(sfp["hydrophobic"]), device=device).bool()
+        self.don = torch.tensor(np.asarray(sfp["donor"]), device=device).bool()
+        self.acc = torch.tensor(np.asarray(sfp["acceptor"]), device=device).bool()
+
+    def prm(self):
+        return tuple(self.p[k] for k in _PRM_KEYS)
+
+    def weights(self, device=None):
+        return torch.tensor([self.p[k] for k in _W_KEYS], device=device or self.radius.device)
+
+    def terms(self, r, ti, tj):
+        return pair_terms(r, ti, tj, self.radius.to(r.device), self.hyd.to(r.device), self.don.to(r.device),
+                          self.acc.to(r.device), self.prm())
+
+    def energy(self, r, ti, tj):
+        return self.terms(r, ti, tj) @ self.weights(r.device).to(r.dtype)
 
 
 class Problem:
+    """Maps + ligand batch + receptor index per ligand + pair potential (+ receptor atoms for exact energies)."""
+
     def __init__(self, gridset, lb, rec_idx, pot, rec=None):
-        self.gs, self.lb, self.rec_idx, self.pot = gridset, lb, rec_idx, pot
-        self.rec = rec  # optional (xyz [R,N,3], types [R,N], mask [R,N]) for exact (grid-free) energies
+        self.gs, self.lb, self.rec_idx, self.pot, self.rec = gridset, lb, rec_idx, pot, rec
 
     def subset(self, idx):
         return Problem(self.gs, self.lb.subset(idx), self.rec_idx[idx], self.pot, self.rec)
 
-    def inter(self, X):
-        lb = self.lb
-        L, M, A, _ = X.shape
-        t = lb.types[:, None, :].expand(L, M, A)
-        ri = self.rec_idx[:, None, None].expand(L, M, A)
-        return self.gs.lookup(X, t, ri, mask=lb.heavy[:, None, :].expand(L, M, A)).sum(-1)
-
-    def inter_exact(self, X):
-        """Direct pairwise ligand-receptor energy (no grid) [L, M] (search.py:73-90)."""
-        rx, rt, rm = self.rec
-        lb = self.lb
-        L, M, A, _ = X.shape
-        out = torch.zeros(L, M, device=X.device, dtype=X.dtype)
-        for l in range(L):
-            ri = int(self.rec_idx[l])
-            hv = lb.heavy[l]
-            xl = X[l][:, hv]
-            tl = lb.types[l][hv]
-            xr, trr = rx[ri][rm[ri]].to(X.dtype), rt[ri][rm[ri]]
-            r = torch.cdist(xl.reshape(-1, 3), xr).reshape(M, xl.shape[1], len(xr))
-            e = self.pot.energy(r, tl[None, :, None].expand_as(r), trr[None, None, :].expand_as(r))
-            out[l] = e.sum((-1, -2))
-        return out
-
-    def intra(self, X):
-        lb = self.lb
-        L, M, A, _ = X.shape
-        pi = lb.pairs[:, None, :, :].expand(L, M, lb.P, 2)
-        xi = torch.gather(X, 2, pi[..., 0:1].expand(L, M, lb.P, 3))
-        xj = torch.gather(X, 2, pi[..., 1:2].expand(L, M, lb.P, 3))
-        r = (xi - xj).norm(dim=-1)
-        ti = torch.gather(lb.types, 1, lb.pairs[..., 0])[:, None].expand(L, M, lb.P)
-        tj = torch.gather(lb.types, 1, lb.pairs[..., 1])[:, None].expand(L, M, lb.P)
-        e = self.pot.energy(r, ti.clamp(min=0), tj.clamp(min=0))
-        e = torch.where(lb.pmask[:, None, :], e, torch.zeros_like(e))
-        return e.sum(-1)
-
-    def energy(self, t, q0, r, theta):
-        """Pose -> (total, inter, intra, coords), torch reference path (search.py:121-126)."""
-        X = pose_coords(self.lb, t, q0, r, theta)
-        ei, ea = self.inter(X), self.intra(X)
-        return ei + ea, ei, ea, X
-
 
 def pad_receptors(receptors, device):
-    """(xyz [R,N,3], types [R,N], mask [R,N]) padded to the largest receptor (search.py:369-379)."""
-    N = max(len(r["rec_xyz"]) for r in receptors)
-    R = len(receptors)
-    xyz = np.zeros((R, N, 3), np.float32)
-    typ = np.zeros((R, N), np.int64)
-    msk = np.zeros((R, N), bool)
-    for i, r in enumerate(receptors):
-        n = len(r["rec_xyz"])
-        xyz[i, :n], typ[i, :n], msk[i, :n] = r["rec_xyz"], r["rec_types"], True
-    T = lambda a: torch.as_tensor(a, device=device)
-    return T(xyz), T(typ), T(msk)
+    """(xyz [R, N, 3] f32, types [R, N] i64, mask [R, N] bool) of receptor dicts padded to the largest."""
+    counts = np.array([len(r["rec_xyz"]) for r in receptors], np.int64)
+    N = int(counts.max())
+    owner = np.repeat(np.arange(len(receptors)), counts)
+    row = np.arange(counts.sum()) - np.repeat(np.cumsum(counts) - counts, counts)
+    xyz = np.zeros((len(receptors), N, 3), np.float32)
+    typ = np.zeros((len(receptors), N), np.int64)
+    xyz[owner, row] = np.concatenate([np.asarray(r["rec_xyz"], np.float32).reshape(-1, 3) for r in receptors])
+    typ[owner, row] = np.concatenate([np.asarray(r["rec_types"], np.int64) for r in receptors])
+    mask = np.arange(N)[None, :] < counts[:, None]
+    return tuple(torch.as_tensor(a, device=device) for a in (xyz, typ, mask))
 
 
-def _bucket(x, step):
-    return max(step, step * math.ceil(x / step))
+def _multiple(x, step):
+    return step * max(1, -(-int(x) // step))
 
 
 def pack_host(prob):
-    """Numpy packing of a Problem for the search kernels. Returns (AM, KM, lig_arrays, sf_arrays) with
-    lig_arrays = [ref, typ, tm, ax, axp, axu, pr, na, nt, np, rg, P, gslot] (mckernel.py:547-599)."""
-    lb, gs, pot = prob.lb, prob.gs, prob.pot
-    preps = lb.preps
+    """Kernel arrays of a Problem: (AM, KM, lig, sf) with
+    lig = [ref, typ, tm, ax, axp, axu, pr, na, nt, np, rg, P, gslot] and sf = [prm (15), radius, hyd, don, acc]."""
+    preps = prob.lb.preps
     L = len(preps)
-    nh = [int(p.heavy.sum()) for p in preps]
-    AM = 64 if max(nh) <= 64 else _bucket(max(nh), 32)
-    KM = _bucket(max(max(p.n_tors for p in preps), 1), 8)
-    P = max(1, max(len(p.pairs) for p in preps))
+    heavy = [np.flatnonzero(np.asarray(p.heavy, bool)) for p in preps]
+    na = np.array([len(h) for h in heavy], np.int32)
+    nt = np.array([p.n_tors for p in preps], np.int32)
+    npr = np.array([len(p.pairs) for p in preps], np.int32)
+    AM = 64 if na.max() <= 64 else _multiple(na.max(), 32)
+    KM = _multiple(max(int(nt.max()), 1), 8)
+    P = max(1, int(npr.max()))
+    # heavy-atom renumbering: new[l][old atom] = position among the ligand's heavy atoms (-1 for hydrogens)
+    new = []
+    for p, h in zip(preps, heavy):
+        m = np.full(p.n, -1, np.int64)
+        m[h] = np.arange(len(h))
+        new.append(m)
+    own_a = np.repeat(np.arange(L), na)
+    pos_a = np.arange(na.sum()) - np.repeat(np.cumsum(na) - na, na)
     ref = np.zeros((L, AM, 3), np.float32)
     typ = np.zeros((L, AM), np.int32)
+    ref[own_a, pos_a] = np.concatenate([np.asarray(p.ref, np.float32)[h] for p, h in zip(preps, heavy)])
+    typ[own_a, pos_a] = np.concatenate([np.asarray(p.types)[h] for p, h in zip(preps, heavy)])
+    # torsions: moved-atom table over heavy atoms, axis atoms renumbered, axis point and unit vector
     tm = np.zeros((L, KM, AM), np.uint8)
     ax = np.zeros((L, KM, 2), np.int32)
     axp = np.zeros((L, KM, 3), np.float32)
     axu = np.zeros((L, KM, 3), np.float32)
+    own_t = np.repeat(np.arange(L), nt)
+    pos_t = np.arange(nt.sum()) - np.repeat(np.cumsum(nt) - nt, nt)
+    if nt.sum():
+        tors = [(np.asarray(p.tors_axis, np.int64).reshape(-1, 2), np.asarray(p.tors_mask, bool).reshape(p.n_tors, p.n))
+                for p in preps]
+        ax_new = np.concatenate([m[a] for (a, _), m in zip(tors, new)])
+        assert (ax_new >= 0).all(), "torsion axis atom is not a heavy atom"
+        ax[own_t, pos_t] = ax_new
+        pa = np.concatenate([np.asarray(p.ref, np.float32)[a[:, 0]] for (a, _), p in zip(tors, preps)])
+        pb = np.concatenate([np.asarray(p.ref, np.float32)[a[:, 1]] for (a, _), p in zip(tors, preps)])
+        axp[own_t, pos_t] = pa
+        axu[own_t, pos_t] = (pb - pa) / np.maximum(np.linalg.norm(pb - pa, axis=1, keepdims=True), np.float32(1e-6))
+        hit = [np.nonzero(msk[:, h]) for (_, msk), h in zip(tors, heavy)]
+        own_h = np.concatenate([np.full(len(k), l) for l, (k, _) in enumerate(hit)])
+        tm[own_h, np.concatenate([k for k, _ in hit]), np.concatenate([a for _, a in hit])] = 1
     pr = np.zeros((L, P, 2), np.int32)
-    na = np.zeros(L, np.int32)
-    nt = np.zeros(L, np.int32)
-    npairs = np.zeros(L, np.int32)
-    rg = np.zeros(L, np.float32)
-    for l, p in enumerate(preps):
-        hv = np.where(p.heavy)[0]
-        remap = -np.ones(p.n, np.int64)
-        remap[hv] = np.arange(len(hv))
-        na[l], nt[l], npairs[l], rg[l] = len(hv), p.n_tors, len(p.pairs), p.rg
-        ref[l, :len(hv)] = p.ref[hv]
-        typ[l, :len(hv)] = p.types[hv]
-        if p.n_tors:
-            tm[l, :p.n_tors, :len(hv)] = p.tors_mask[:, hv]
-            ax[l, :p.n_tors] = remap[p.tors_axis]
-            assert (ax[l, :p.n_tors] >= 0).all(), "torsion axis atom is not a heavy atom"
-            pa, pb = p.ref[p.tors_axis[:, 0]], p.ref[p.tors_axis[:, 1]]
-            u = pb - pa
-            axp[l, :p.n_tors] = pa
-            axu[l, :p.n_tors] = u / np.maximum(np.linalg.norm(u, axis=1, keepdims=True), 1e-6)
-        if len(p.pairs):
-            pr[l, :len(p.pairs)] = remap[p.pairs]
-    slot = gs.slot.cpu().numpy()
-    ri_np = prob.rec_idx.cpu().numpy()
+    if npr.sum():
+        own_p = np.repeat(np.arange(L), npr)
+        pos_p = np.arange(npr.sum()) - np.repeat(np.cumsum(npr) - npr, npr)
+        pr[own_p, pos_p] = np.concatenate([m[np.asarray(p.pairs, np.int64).reshape(-1, 2)]
+                                           for p, m in zip(preps, new) if len(p.pairs)])
+    rg = np.array([p.rg for p in preps], np.float32)
+    # grid slot of each heavy atom in its receptor's maps
+    slot = prob.gs.slot.cpu().numpy() if torch.is_tensor(prob.gs.slot) else np.asarray(prob.gs.slot)
+    rec = np.asarray(prob.rec_idx.cpu() if torch.is_tensor(prob.rec_idx) else prob.rec_idx, np.int64)
     gsl = np.zeros((L, AM), np.int32)
-    for l in range(L):
-        gsl[l, :na[l]] = slot[ri_np[l], typ[l, :na[l]]]
+    gsl[own_a, pos_a] = slot[rec[own_a], typ[own_a, pos_a]]
     assert (gsl >= 0).all(), "a ligand atom type has no grid"
-    lig = [ref, typ, tm, ax, axp, axu, pr, na, nt, npairs, rg, np.int32(P), gsl]
-    sp = pot.p
-    prm = np.array([sp["g1_off"], sp["g1_w"], sp["g2_off"], sp["g2_w"], sp["rep_off"], sp["hyd_good"],
-                    sp["hyd_bad"], sp["hb_good"], sp["hb_bad"], sp["cutoff"], sp["w_g1"], sp["w_g2"],
-                    sp["w_rep"], sp["w_hyd"], sp["w_hb"]], np.float32)
+    lig = [ref, typ, tm, ax, axp, axu, pr, na, nt, npr, rg, np.int32(P), gsl]
+    sp = prob.pot.p
+    prm = np.array([sp[k] for k in _PRM_KEYS + _W_KEYS], np.float32)
     sf = [prm, np.asarray(sp["radius"], np.float32), np.asarray(sp["hydrophobic"], np.int32),
           np.asarray(sp["donor"], np.int32), np.asarray(sp["acceptor"], np.int32)]
     return AM, KM, lig, sf
 
 
-def heavy_index(lb, AM):
-    """[L, AM] index of each packed heavy atom in the LigandBatch atom order (0 past the end)."""
-    L = lb.L
-    hidx = torch.zeros(L, AM, dtype=torch.long, device=lb.ref.device)
-    for l, p in enumerate(lb.preps):
-        hv = torch.as_tensor(np.where(p.heavy)[0], device=lb.ref.device)
-        hidx[l, :len(hv)] = hv
-    return hidx
-
-
-__all__ = ["Problem", "PairPotential", "pair_terms", "pad_receptors", "pack_host", "heavy_index", "internal_coords",
-           "pose_coords"]
+__all__ = ["Problem", "PairPotential", "pair_terms", "pad_receptors", "pack_host"]

@@ -17,6 +17,7 @@ from __future__ import annotations
 
 import math
 
+import numpy as np
 import torch
 
 from . import _lib
@@ -29,6 +30,13 @@ def _gemm(A, sA, B, sB, M, N, K, C=None, beta=0.0, bias=None, act=0, pre=None, C
     _lib.call("adock_gemm_bf16", M, N, K, _lib.ptr(A), sA[0], sA[1], _lib.ptr(B), sB[0], sB[1], _lib.ptr(C),
               N if C is not None else 0, float(beta), _lib.ptr(bias), int(act), _lib.ptr(pre), _lib.ptr(Cb),
               N if Cb is not None else 0, _lib.stream_ptr())
+
+
+def check_gemm(where):
+    """Raise if a tensor-core GEMM gave up waiting for its MMAs since the last check (its output tile was then not
+    written, so the network's outputs or gradients are unusable). Synchronises the device."""
+    if _lib.load().adock_gemm_status() != 0:
+        raise RuntimeError(f"{where}: a tcgen05 GEMM timed out waiting for its tensor-core work; results discarded")
 
 
 class ProposalNet:
@@ -135,6 +143,7 @@ class ProposalNet:
                 tot += self.train_step(X[idx].contiguous(), Y[idx].contiguous(), lr=lr)
                 nb += 1
             last = float(tot) / max(nb, 1)
+            check_gemm(f"training epoch {ep}")
             if log is not None:
                 log(f"epoch {ep}: loss {last:.4f}")
         return last
@@ -225,18 +234,13 @@ def collect_learned(kp, net, chain_lig, chain_id, cur, cfg, seed, cap, prop_k=32
 
 def _starts(prob, kp, cfg, seed):
     """Stage-A start poses of every chain (the search driver's first stage), packed as MC states."""
-    from .search import stage_a_kernel
+    from .search import stage_a_starts
     dev = kp.device
     L, M = prob.lb.L, cfg["n_chains"]
-    gen = torch.Generator(device=dev)
-    gen.manual_seed(seed)
-    bc = ((prob.gs.lo[0] + prob.gs.hi[0]) / 2)[None].expand(L, 3)
-    bs = [(prob.gs.hi[0] - prob.gs.lo[0]).cpu().numpy()] * L
-    t, q0, th, _ = stage_a_kernel(prob, kp, bc, bs, cfg, gen)
-    N = L * M
-    cur = kp.pack(t.reshape(N, 3), q0.reshape(N, 4), th.reshape(N, -1))
+    lo, hi = prob.gs.lo[0].cpu().numpy(), prob.gs.hi[0].cpu().numpy()
+    cur, _ = stage_a_starts(prob, kp, np.tile((lo + hi) / 2, (L, 1)), [hi - lo] * L, cfg, seed)
     chain_lig = torch.arange(L, device=dev, dtype=torch.int32).repeat_interleave(M)
-    chain_id = torch.arange(N, device=dev, dtype=torch.int32)
+    chain_id = torch.arange(L * M, device=dev, dtype=torch.int32)
     return chain_lig, chain_id, cur
 
 
@@ -432,6 +436,7 @@ def run_mc_segments(kp, net, chain_lig, chain_id, cur, cur_e, best, best_e, cfg,
         kp.run_mc(chain_lig, chain_id, cur, cur_e, best, best_e, init_opt and sg == 0, k, cfg["bfgs_iters"],
                   cfg["mc_temperature"], cfg["mc_amp_pos"], cfg["mc_amp_rot"], seed, sg * prop_k, prop=moves,
                   prop_stats=pst, prop_frac=prop_frac, log=log)
+    check_gemm("learned-proposal search")
     if stats is not None:
         p, pa, q, qa = pst.tolist()
         stats.update(prop_steps=p, prop_accepted=pa, plain_steps=q, plain_accepted=qa)

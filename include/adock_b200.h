@@ -129,6 +129,8 @@ typedef struct {
     int* log_n;
     int log_cap;
     float prop_frac;           /* with proposals: fraction of steps that take the learned move (<= 0 or >= 1: all) */
+    const int* lig_active;     /* dev [L] or NULL: chains of ligands whose flag is 0 are skipped (left unchanged);
+                                  replaces the host-side compaction of active chains (search.py:614-627) */
 } adock_mc_args_t;
 
 /* ------------------------------------------------------------------------------------------------ misc */
@@ -181,6 +183,61 @@ int adock_mc(const adock_ligands_t* lig, const adock_work_t* work, const adock_g
 int adock_stage_a(const adock_ligands_t* lig, const adock_work_t* work, const adock_grids_t* grids,
                   const adock_sf_t* sf, const float* conf, int C, const float* quats, int Q, const float* trans,
                   const int* ntrans, int nt_max, float cap, float* best_e, int* best_i, void* stream);
+
+/* adock_stage_a with the translation lattices per box instead of per ligand: trans [B, nt_max, 3], ntrans [B]
+ * and lig_box [L] (dev), so ligands docked into one box share one lattice. Same kernel as adock_stage_a. */
+int adock_stage_a_boxes(const adock_ligands_t* lig, const adock_work_t* work, const adock_grids_t* grids,
+                        const adock_sf_t* sf, const float* conf, int C, const float* quats, int Q, const float* trans,
+                        const int* ntrans, int nt_max, const int* lig_box, float cap, float* best_e, int* best_i,
+                        void* stream);
+
+/* ---- device-side search pipeline: the host glue of the reference search (search.py:322-366, 506-537, 614-636)
+ * as kernels, so that a whole search runs on one stream without host round trips. */
+
+/* Stage-A conformers: replaces the torch conformer sampling of stage_a_kernel (search.py:329-337). Per ligand NT
+ * torsion sets (set 0 = the input conformer; the others uniform in [-pi, pi) from a counter-based stream of
+ * (seed, ligand, set, torsion)), their intra-ligand energy, and the C of lowest energy (ties: lower set index) in
+ * ascending order: theta [L, C, KM], heavy-atom ligand-frame coordinates conf [L, C, AM, 3], energies e [L, C]
+ * (dev). NT <= 4096, C <= NT. */
+int adock_conformers(const adock_ligands_t* lig, const adock_work_t* work, const adock_sf_t* sf, int NT, int C,
+                     unsigned long long seed, float* theta, float* conf, float* e, void* stream);
+
+/* Stage-A translation lattice: replaces search.py:346-353. Per box b (box [B, 6] = centre xyz, size xyz;
+ * receptor box_rec [B]; map slot of the probe type box_slot [B]; points per axis box_n [B, 3], all dev) the
+ * points centre - size/2 + 1 + i * step whose nearest-grid probe energy plus out-of-box penalty is <= probe_max,
+ * in lattice order (x slowest), into trans [B, nt_max, 3]; counts ntrans [B]; the box centre alone when no point
+ * passes. */
+int adock_lattice(const adock_grids_t* grids, int B, const float* box, const int* box_rec, const int* box_slot,
+                  const int* box_n, float step, float probe_max, int nt_max, float* trans, int* ntrans, void* stream);
+
+/* Start states: replaces search.py:356-366. Per ligand the M lowest of best_e[l, j] + e_conf[l, j / Q] over
+ * j < C*Q (ties: lower j; cycled when C*Q < M); state [L*M, 7+KM] = (trans[lig_box[l], best_i[l, j]],
+ * quats[j % Q], theta[l, j / Q]); e_start [L*M] the sorted totals (may be NULL). lig_box may be NULL (box = l).
+ * C*Q <= 16384. */
+int adock_select_starts(int L, int C, int Q, int KM, int M, const float* best_e, const int* best_i,
+                        const float* e_conf, const float* quats, const float* theta, const float* trans,
+                        const int* lig_box, int nt_max, float* state, float* e_start, void* stream);
+
+/* Per-segment bookkeeping of the MC phase: replaces the host logic of search.py:615-636. After segment sg of
+ * `seg` steps (chains ligand-major, M per ligand): *chain_steps += M * seg per active ligand (may be NULL); per
+ * ligand glob = min(glob, best over its chains), stall = 0 if that improved glob by more than es_tol else +1,
+ * active &= seg_lim > next_sg && (es_rounds <= 0 || stall < es_rounds). All arrays dev. */
+int adock_segment_update(int L, int M, int seg, int next_sg, int es_rounds, float es_tol, const float* best_e,
+                         const int* seg_lim, float* glob, int* stall, int* active, unsigned long long* chain_steps,
+                         void* stream);
+
+/* Greedy clustering of the final poses: replaces search.py:516-531. Per ligand its P poses (e_total [L*P],
+ * heavy-atom coordinates X [L*P, AM, 3], dev) in ascending energy order (ties: lower index); a pose becomes a
+ * representative when its heavy-atom RMSD to every earlier one is >= cut, until n_out are found:
+ * reps [L, n_out] (pose index within the ligand, -1 past n_reps[l]). P <= 4096, n_out <= 32. */
+int adock_cluster(const adock_work_t* work, int L, int P, const double* e_total, const float* X, int AM, float cut,
+                  int n_out, int* reps, int* n_reps, void* stream);
+
+/* All-atom world coordinates of n states: replaces ligand.pose_coords (ligand.py:216-237) for the returned poses.
+ * ref_all [L, A, 3] ligand-frame coordinates of every atom (hydrogens included), mask_all [L, A] torsion bitmask
+ * of each atom (bit k: torsion k moves it), torsion axes from `work`; X [n, A, 3] (all dev). */
+int adock_pose_atoms(const adock_work_t* work, int KM, const float* ref_all, const unsigned* mask_all, int A,
+                     const int* chain_lig, int n, const float* state, float* X, void* stream);
 
 /* Receptor neighbour lists: replaces KernelProblem.receptor_neighbours (mckernel.py:662-688).
  * Pass 1 (nbr == NULL): counts [N] of receptor atoms within `cut` of any heavy atom of each chain's pose.

@@ -12,7 +12,8 @@ Flags: the reference uses ``-O3 -march=native -ffast-math -fopenmp``; ``-march=n
 ``-march=x86-64-v3`` because the built library travels to other hosts.
 
 Outputs only into ``oracle/_ref/``. Test infrastructure: nothing in the product imports this.
-Usage: ``python oracle/build_ref.py [--reference DIR]`` (default ``$ADOCK_REFERENCE`` or /root/reference).
+Usage: ``python oracle/build_ref.py [--reference DIR]``. Without the argument the checkout is ``$ADOCK_REFERENCE``,
+else the read-only mount of the build container (``CONTAINER_MOUNT``); ``locate_reference`` resolves it.
 """
 import argparse
 import os
@@ -23,6 +24,16 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
+CONTAINER_MOUNT = Path("/root/reference")   # where the build container mounts the reference checkout
+
+
+def locate_reference(arg=None):
+    """The reference checkout to build from (argument, then $ADOCK_REFERENCE, then the container mount), or None
+    when none of them holds one."""
+    for cand in (arg, os.environ.get("ADOCK_REFERENCE"), CONTAINER_MOUNT):
+        if cand and (Path(cand) / "src" / "adock" / "cpukernel.py").exists():
+            return Path(cand)
+    return None
 BUCKETS = [(64, 8), (64, 16), (64, 24), (96, 8), (96, 16), (96, 24)]
 CXXFLAGS = ["-O3", "-march=x86-64-v3", "-ffast-math", "-ffp-contract=off", "-fopenmp", "-fPIC", "-shared", "-std=c++17", "-w"]
 
@@ -84,8 +95,11 @@ def build(ref: Path, force: bool = False) -> list:
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("ADOCK_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", default=None)
     ap.add_argument("--force", action="store_true")
     a = ap.parse_args()
-    for p in build(Path(a.reference), a.force):
+    ref = locate_reference(a.reference)
+    if ref is None:
+        ap.error("no reference checkout: give --reference DIR or set ADOCK_REFERENCE")
+    for p in build(ref, a.force):
         print(p)

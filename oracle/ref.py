@@ -252,28 +252,28 @@ class RefKernelProblem:
                        None if nbr is None else nbr.numpy(), None if nbr_n is None else nbr_n.numpy())
 
     def receptor_neighbours(self, prob, chain_lig, states, K, margin):
+        """Per chain: receptor atoms within cutoff + margin of any heavy atom of the pose, in receptor order."""
+        import numpy as np
+        from adock_b200.problem import pack_host
+        from oracle.fp64 import Packed
         torch = self._torch
-        from adock_b200.ligand import pose_coords
         rx, rt, rm = prob.rec
-        lb = prob.lb
         cut = float(prob.pot.p["cutoff"]) + margin
-        N = states.shape[0]
-        lists = []
-        cl = chain_lig.long()
-        for l in torch.unique(cl).tolist():
-            idx = (cl == l).nonzero().squeeze(1)
-            t, q, th = self.unpack(states[idx], K)
-            sub = lb.subset(torch.tensor([l]))
-            X = pose_coords(sub, t[None], q[None], torch.zeros_like(t)[None], th[None])[0][:, lb.heavy[l]]
+        AM, KM, lig, sf = pack_host(prob)
+        model = Packed(lig, sf)
+        st = states.double().numpy()
+        cl = chain_lig.long().numpy()
+        near_all = []
+        for n in range(len(st)):
+            l = int(cl[n])
+            X = model.pose_heavy(l, st[n:n + 1])[0]
             ri = int(prob.rec_idx[l])
-            xr = rx[ri][rm[ri]]
-            near = (torch.cdist(X.reshape(-1, 3), xr).view(len(idx), -1, len(xr)) < cut).any(1)
-            lists.append((idx, near))
-        NB = max(1, max(int(n.sum(1).max()) for _, n in lists))
-        nbr = torch.zeros(N, NB, dtype=torch.int32)
-        nbr_n = torch.zeros(N, dtype=torch.int32)
-        for idx, near in lists:
-            order = torch.argsort((~near).to(torch.int8), dim=1, stable=True)[:, :NB]
-            nbr[idx, :order.shape[1]] = order.to(torch.int32)
-            nbr_n[idx] = near.sum(1).to(torch.int32)
+            xr = rx[ri][rm[ri]].double().numpy()
+            near_all.append(np.flatnonzero((np.linalg.norm(X[:, None] - xr[None], axis=-1) < cut).any(0)))
+        NB = max(1, max(len(x) for x in near_all))
+        nbr = torch.zeros(len(st), NB, dtype=torch.int32)
+        nbr_n = torch.zeros(len(st), dtype=torch.int32)
+        for n, near in enumerate(near_all):
+            nbr[n, :len(near)] = torch.as_tensor(near, dtype=torch.int32)
+            nbr_n[n] = len(near)
         return nbr, nbr_n

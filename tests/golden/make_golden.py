@@ -1,9 +1,9 @@
 """Generate the golden fixtures in tests/golden/ from the reference implementation itself.
 
-Run where a reference checkout is present:  python tests/golden/make_golden.py [--reference DIR]
-The reference package is imported unmodified with empty stand-ins for ``cupy`` and ``rdkit`` (its CPU path and
-the functions used here do not touch them); its host kernels are compiled by its own ``adock.cpukernel``
-(cache directory under this repository's ``_work/``). The synthetic inputs come from ``adock_b200.synth`` with
+Run where a reference checkout is present:  python tests/golden/make_golden.py --reference DIR
+(or with ADOCK_REFERENCE=DIR). The reference package is imported unmodified with empty stand-ins for ``cupy`` and
+``rdkit`` (its CPU path and the functions used here do not touch them); its host kernels are compiled by its own
+``adock.cpukernel`` into a temporary cache directory. The synthetic inputs come from ``adock_b200.synth`` with
 fixed seeds, so every fixture records (inputs, reference outputs). Fixtures:
 
   pack.npz        reference mckernel.pack_host of a 3-ligand synthetic batch
@@ -11,6 +11,11 @@ fixed seeds, so every fixture records (inputs, reference outputs). Fixtures:
   fitted.npz      reference fit.terms Spec/FittedPotential: W table, radii, grid prm, features of 3 known pairs
   grid.npz        reference cpukernel.build_grid_cpu maps (small receptor, ragged 13x15x17, 4 types, per_term too)
   search.npz      reference CpuKernelProblem: energy_grad (grid + exact) of 32 poses, stage_a, one MC step
+  batch.npz       reference ligand.LigandBatch padded arrays of the 3-ligand batch
+  finalize.npz    reference search.finalize_kernel on fixed final states (12 per ligand, in near-duplicate groups):
+                  per-state exact totals, the representatives it picks and its result arrays
+  dock.npz        reference search.dock_problem_kernel (device "cpu"): 3 small ligands against the config-0
+                  receptor, 16 chains x 300 steps, seeds 0-7: best affinity per (seed, ligand)
 """
 import argparse
 import os
@@ -26,10 +31,11 @@ sys.path.insert(0, str(ROOT))
 
 
 def _import_reference(ref):
+    import tempfile
     for name in ("cupy", "rdkit", "rdkit.Chem"):
         sys.modules.setdefault(name, types.ModuleType(name))
     sys.modules["rdkit"].Chem = sys.modules["rdkit.Chem"]
-    os.environ.setdefault("ADOCK_CPU_CACHE", str(ROOT / "_work" / "ref_cpu_cache"))
+    os.environ.setdefault("ADOCK_CPU_CACHE", tempfile.mkdtemp(prefix="adock_ref_cpu_"))
     sys.path.insert(0, str(Path(ref) / "src"))
     import torch  # noqa: F401
     from adock import config, cpukernel, grid, ligand, mckernel, scoring, search
@@ -146,11 +152,70 @@ def main(ref):
                         e_exact=ex.numpy(), g_exact=gx.numpy(), conf=conf.numpy(), quats=quats.numpy(),
                         trans=trans.numpy(), ntrans=ntr.numpy(), stage_e=be.numpy(), stage_i=bi.numpy(),
                         mc_chain_id=ci.numpy(), mc_cur=cur.numpy(), mc_cur_e=cur_e.numpy(), mc_best_e=best_e.numpy())
+    # ---------------- LigandBatch arrays ----------------
+    names = ["ref", "types", "amask", "axis", "tmask", "tvalid", "pairs", "pmask", "rg", "n_tors_vina", "axis_p",
+             "axis_u"]
+    np.savez_compressed(HERE / "batch.npz", **{k: getattr(lb, k).numpy() for k in names})
+
+    # ---------------- finalize on fixed states ----------------
+    # per ligand 4 base poses x 3 near-duplicates (0.2 A translation jitter): the greedy 2 A clustering must keep
+    # one representative per group
+    P, groups = 12, 4
+    L = len(ligs)
+    tb = c + torch.randn((L, groups, 1, 3), generator=g) * 1.5
+    qb = R["ligand"].random_quat((L, groups, 1), g, "cpu")
+    thb = (torch.rand((L, groups, 1, lb.K), generator=g) * 2 - 1) * np.pi
+    t = (tb + torch.randn((L, groups, 3, 3), generator=g) * 0.2).reshape(L * P, 3)
+    q = qb.expand(L, groups, 3, 4).reshape(L * P, 4)
+    th = (thb.expand(L, groups, 3, lb.K) * lb.tvalid[:, None, None, :]).reshape(L * P, lb.K)
+    fst = kp.pack(t, q, th)
+    fcl = torch.arange(L, dtype=torch.int32).repeat_interleave(P)
+    fe, _ = kp.energy_grad(fcl, fst, exact=True)
+    cfg_f = dict(cfg["search"]["v2_default"])
+    res = R["search"].finalize_kernel(prob, kp, fst, fcl, L, P, cfg_f)
+    reps, out = [], {}
+    for l, r in enumerate(res):
+        # the representative states, recovered from their (exactly equal) totals
+        el = fe.view(L, P)[l].numpy()
+        reps.append([int(np.flatnonzero(el == v)[0]) for v in r["total"]])
+    out["counts"] = np.array([len(r["affinity"]) for r in res])
+    for k in ("affinity", "inter", "intra", "total"):
+        out[k] = np.concatenate([r[k] for r in res])
+    out["coords"] = np.concatenate([r["coords"] for r in res])
+    np.savez_compressed(HERE / "finalize.npz", state=fst.numpy(), chain_lig=fcl.numpy(), P=P, e_exact=fe.numpy(),
+                        reps=np.concatenate(reps), cluster_rmsd=cfg_f["cluster_rmsd"], n_out=cfg_f["n_out"], **out)
+
+    # ---------------- the whole search on the host cores, several seeds ----------------
+    # the config-0 receptor (1,500 atoms, 22.5 A box) and three small ligands, where independent searches converge
+    from adock_b200 import synth
+    rec0 = synth.config_receptor(0)
+    ligs0 = [synth.ligand(n, r, sd) for n, r, sd in ((12, 2, 101), (16, 3, 102), (20, 4, 103))]
+    L0 = len(ligs0)
+    t0 = np.unique(np.concatenate([[0]] + [l.types for l in ligs0]))
+    gs0 = R["grid"].make_gridset([rec0], sfp, 0.375, 10.0, device="cpu", lig_types=[t0])
+    prob0 = R["search"].Problem(gs0, R["ligand"].LigandBatch(ligs0, "cpu"), torch.zeros(L0, dtype=torch.long),
+                                R["scoring"].PairPotential(sfp), rec=R["search"].pad_receptors([rec0], "cpu"))
+    cfg_d = dict(cfg["search"]["v2_default"], n_chains=16, mc_steps=300, mc_segment=300, mc_size_ref=0,
+                 min_total_chains=0)
+    bc = torch.tensor(rec0["center"], dtype=torch.float32)[None].expand(L0, 3)
+    bs = [rec0["size"]] * L0
+    seeds = list(range(8))
+    best = np.zeros((len(seeds), L0))
+    for i, sd in enumerate(seeds):
+        r = R["search"].dock_problem_kernel(prob0, bc, bs, cfg_d, seed=sd)
+        best[i] = [float(np.min(x["affinity"])) for x in r]
+    np.savez_compressed(HERE / "dock.npz", seeds=np.array(seeds), best_affinity=best,
+                        ligands=np.array([[12, 2, 101], [16, 3, 102], [20, 4, 103]]), n_chains=cfg_d["n_chains"],
+                        mc_steps=cfg_d["mc_steps"])
     for f in sorted(HERE.glob("*.npz")):
         print(f.name, f.stat().st_size)
 
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("ADOCK_REFERENCE", "/root/reference"))
-    main(ap.parse_args().reference)
+    ap.add_argument("--reference", default=os.environ.get("ADOCK_REFERENCE"),
+                    help="reference checkout (default: $ADOCK_REFERENCE)")
+    a = ap.parse_args()
+    if not a.reference:
+        ap.error("give --reference DIR or set ADOCK_REFERENCE")
+    main(a.reference)

@@ -8,7 +8,7 @@ import torch
 
 from adock_b200 import params, synth
 from adock_b200.grid import GridSet, grid_dims
-from adock_b200.ligand import LigandBatch, random_quat
+from adock_b200.ligand import LigandBatch
 from adock_b200.problem import PairPotential, Problem, pack_host, pad_receptors
 
 SPACING = params.GRID_SPACING
@@ -71,6 +71,12 @@ def oracle_problem(prob):
                 dims=gs.dims.cpu().numpy(), T=gs.T, spacing=gs.spacing, penalty=gs.penalty)
     rx, rt, rm = prob.rec
     return R.RefProblem(AM, KM, lig, sf, grid, rec=(rx.cpu().numpy(), rt.cpu().numpy(), rm.sum(1).cpu().numpy()))
+
+
+def random_quat(shape, gen, device="cpu"):
+    """Unit quaternions [*shape, 4] (w, x, y, z), uniform on the 3-sphere (normalised Gaussians)."""
+    q = torch.randn(tuple(shape) + (4,), generator=gen, device=device)
+    return q / q.norm(dim=-1, keepdim=True)
 
 
 def random_states(prob, n_per_lig, seed=0, sigma=1.5):

@@ -43,6 +43,54 @@ def _golden_problem():
     return prob
 
 
+def test_ligand_batch_matches_reference():
+    """LigandBatch's padded arrays equal the reference LigandBatch's on the golden ligands (and its per-atom torsion
+    bitmasks, the all-atom kinematics' input, encode the same moved-atom table)."""
+    from adock_b200.ligand import LigandBatch
+    gold = _load("batch.npz")
+    lb = LigandBatch(_golden_ligands())
+    for k, v in gold.items():
+        got = getattr(lb, k).numpy()
+        assert got.shape == v.shape, k
+        if v.dtype.kind == "f":
+            np.testing.assert_allclose(got, v, rtol=1e-6, atol=1e-7, err_msg=k)
+        else:
+            np.testing.assert_array_equal(got, v, err_msg=k)
+    bits = lb.atom_masks()
+    table = (bits[:, None, :] >> np.arange(lb.K, dtype=np.uint32)[None, :, None]) & 1
+    np.testing.assert_array_equal(table.astype(bool), gold["tmask"])
+    sub = lb.subset(torch.tensor([2, 0]))
+    np.testing.assert_array_equal(sub.ref.numpy(), gold["ref"][[2, 0]])
+    np.testing.assert_array_equal(sub.atom_masks(), bits[[2, 0]])
+
+
+def test_search_host_tables():
+    """The search driver's host tables: one lattice per distinct (receptor, box), its point counts per axis (those
+    of arange(-s/2 + 1, s/2 - 1 + 1e-6, step)), the box of each ligand, and the chain widening rule."""
+    from adock_b200.search import _boxes, _widen
+    from adock_b200 import params
+
+    class _Prob:
+        class lb:
+            L = 4
+        rec_idx = torch.tensor([0, 0, 1, 0])
+
+    c = torch.tensor([[1.0, 2, 3], [1.0, 2, 3], [1.0, 2, 3], [0.0, 0, 0]])
+    s = [np.array([22.5, 22.5, 22.5])] * 3 + [np.array([10.0, 12.0, 14.5])]
+    table, rec, n, lig_box = _boxes(_Prob, c, s, 1.5)
+    assert len(table) == 3 and lig_box[0] == lig_box[1] and len({lig_box[0], lig_box[2], lig_box[3]}) == 3
+    for b in range(3):
+        l = int(np.flatnonzero(lig_box == b)[0])
+        np.testing.assert_allclose(table[b], np.concatenate([c[l].numpy(), s[l]]))
+        assert rec[b] == int(_Prob.rec_idx[l])
+        want = [len(np.arange(-x / 2 + 1.0, x / 2 - 1.0 + 1e-6, 1.5)) for x in s[l]]
+        np.testing.assert_array_equal(n[b], want)
+    cfg = dict(params.V2_DEFAULT)
+    wide, f = _widen(cfg, 4)
+    assert f == 4 and wide["n_chains"] == 1024 and wide["mc_steps"] == 32 and wide["mc_segment"] == 8
+    assert _widen(cfg, 64)[1] == 1
+
+
 def test_pack_host_matches_reference():
     from adock_b200.problem import pack_host
     gold = _load("pack.npz")

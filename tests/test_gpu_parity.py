@@ -75,6 +75,39 @@ def test_grid_fit_matches_oracle(dev):
         assert rel_close(G, R, 1e-5) < 1e-5
 
 
+@pytest.mark.parametrize("case", ["stock", "buried_charged", "dense"])
+def test_grid_fit_config2_matches_oracle(dev, case):
+    """Fitted maps at the config-2 size (8,000-atom receptor, 30 A box, 81^3 points, 8 ligand types) against the
+    reference's own fitted kernel built on the host: the stock preset (buriedness threshold 177, no charges); a
+    threshold of 120 with receptor charges and charged ligand types (buried and charged receptor ext types, the
+    ionic basis); and a dense receptor whose tiles hold more atoms than one shared-memory staging pass."""
+    _need_oracle()
+    from adock_b200 import params, synth
+    from adock_b200.grid import build_grid_fit
+    X = params.N_XS
+    if case == "dense":
+        xyz, ty = synth.receptor(8000, 26.0, min_sep=1.2, seed=4)
+        rec = synth.receptor_dict(xyz, ty, np.full(3, 13.0), np.full(3, 12.0))
+        n = 33
+    else:
+        rec, n = synth.config_receptor(2), 81
+    spec = params.fitted_spec() if case != "buried_charged" else params.FittedSpec("vina", buried_threshold=120.0)
+    rng = np.random.default_rng(7)
+    chg = rng.choice([0, 1, 2], len(rec["rec_xyz"]), p=[0.8, 0.1, 0.1]) if case == "buried_charged" else None
+    rext = params.receptor_ext_types(rec["rec_xyz"], rec["rec_types"], spec, rec_chg=chg)
+    lig_list = (np.array([0, 1, 2, 3, 4, 8, 9, 10]) if case != "buried_charged"
+                else np.array([0, 1, 3 + X, 4 + 2 * X, 8, 9 + X, 10 + 2 * X, 2]))
+    if case == "buried_charged":
+        assert (rext >= X).sum() > 500 and (rext >= 2 * X).sum() > 500
+    pot = params.FittedPotential(spec, params.fitted_weights(), lig_list)
+    o = rec["center"] - rec["size"] / 2
+    G = build_grid_fit(rec["rec_xyz"], rext, pot, o, SPACING, n, device=dev).cpu().numpy()
+    Rf = oracle_ref.build_grid_fit(rec["rec_xyz"], rext, pot.W, spec.rec_radius, pot.radius, spec.grid_prm(), o,
+                                   SPACING, n)
+    assert G.shape == Rf.shape == (8, n, n, n)
+    assert rel_close(G, Rf, 1e-5) < 1e-5
+
+
 def _problems(dev, sf="vina", kind="mixed"):
     from adock_b200 import params
     sfp = params.sf_params(sf)
@@ -107,7 +140,7 @@ def test_energy_gradient_matches_oracle(dev, sf, exact, kind):
 def test_stage_a_matches_oracle(dev):
     _need_oracle()
     from adock_b200.kernel import B200KernelProblem
-    from adock_b200.ligand import random_quat
+    from helpers import random_quat
     pg, pc = _problems(dev)
     kp = B200KernelProblem(pg)
     rp = oracle_problem(pc)
@@ -201,22 +234,19 @@ def test_mc_lowers_energy_and_best_is_consistent(dev):
     assert float(best_e.median()) < float(e0.median())
 
 
-def test_neighbours_match_torch(dev):
+def test_neighbours_match_fp64_oracle(dev):
     from adock_b200.kernel import B200KernelProblem
-    from adock_b200.ligand import pose_coords
+    from adock_b200.problem import pack_host
+    from oracle.fp64 import Packed
     pg, pc = _problems(dev, kind="mixed")
     kp = B200KernelProblem(pg)
     cl, st = random_states(pc, 8, seed=5)
     nbr, cnt = kp.receptor_neighbours(pg, torch.as_tensor(cl, device=dev), torch.as_tensor(st, device=dev), pg.lb.K, 2.0)
+    model = Packed(*pack_host(pc)[2:])
     rx = pc.rec[0][0].numpy()
     cut = 8.0 + 2.0
     for i in range(len(cl)):
-        l = cl[i]
-        t, q, th = (torch.as_tensor(st[i:i + 1, :3]), torch.as_tensor(st[i:i + 1, 3:7]),
-                    torch.as_tensor(st[i:i + 1, 7:7 + pc.lb.K]))
-        sub = pc.lb.subset(torch.tensor([l]))
-        X = pose_coords(sub, t[None], q[None], torch.zeros_like(t)[None], th[None])[0, 0].numpy()
-        X = X[:pc.lb.preps[l].n][pc.lb.preps[l].heavy]
+        X = model.pose_heavy(int(cl[i]), st[i:i + 1])[0]
         d = np.linalg.norm(X[:, None] - rx[None], axis=-1).min(0)
         want = np.where(d < cut)[0]
         border = np.abs(d - cut) < 1e-4
@@ -225,30 +255,38 @@ def test_neighbours_match_torch(dev):
         assert np.all(np.diff(got) > 0)
 
 
-def test_rescore64_matches_torch_fp64(dev):
+def _fp64_energies(pc, cl, st, exact, maps=None):
+    """Float64 oracle totals and intra energies of states (grid mode on `maps`, default the problem's)."""
+    from adock_b200.problem import pack_host
+    from oracle.fp64 import Packed
+    model = Packed(*pack_host(pc)[2:])
+    gs = pc.gs
+    lo, hi = gs.lo[0].numpy(), gs.hi[0].numpy()
+    G = (gs.flat.double().numpy().reshape(-1, *gs.dims[0].tolist()) if maps is None else maps)
+    tot, intra = np.zeros(len(cl)), np.zeros(len(cl))
+    for l in np.unique(cl):
+        sel = np.where(cl == l)[0]
+        X = model.pose_heavy(int(l), st[sel])
+        inter = (model.exact_inter(int(l), X, pc.rec[0][0].numpy(), pc.rec[1][0].numpy()) if exact
+                 else model.grid_inter(int(l), X, G, gs.origin[0].numpy(), gs.spacing))
+        ia = model.intra(int(l), X)
+        tot[sel] = inter + model.penalty(X, lo, hi, gs.penalty) + ia
+        intra[sel] = ia
+    return tot, intra
+
+
+@pytest.mark.parametrize("exact", [True, False])
+def test_rescore64_matches_fp64_oracle(dev, exact):
+    """The float64 device re-score (finalize's energies, and the yardstick of the map-precision report in grid
+    mode) against the float64 numpy oracle: exact pairwise and grid (trilinear of the FP32 maps) modes."""
     from adock_b200.kernel import B200KernelProblem
-    from adock_b200.ligand import LigandBatch
-    from adock_b200.problem import Problem
     pg, pc = _problems(dev, kind="mixed")
     kp = B200KernelProblem(pg)
     cl, st = random_states(pc, 16, seed=6, sigma=1.0)
-    et, ei, X = kp.rescore64(torch.as_tensor(cl, device=dev), torch.as_tensor(st, device=dev), exact=True)
-    lb64 = pc.lb.to(torch.float64)
-    p64 = Problem(pc.gs, lb64, pc.rec_idx, pc.pot, pc.rec)
-    L, M = pc.lb.L, 16
-    t = torch.as_tensor(st[:, :3], dtype=torch.float64).view(L, M, 3)
-    q = torch.as_tensor(st[:, 3:7], dtype=torch.float64).view(L, M, 4)
-    th = torch.as_tensor(st[:, 7:7 + pc.lb.K], dtype=torch.float64).view(L, M, -1)
-    from adock_b200.ligand import pose_coords
-    Xr = pose_coords(lb64, t, q, torch.zeros_like(t), th)
-    inter = p64.inter_exact(Xr)
-    # out-of-box penalty as in the grid path
-    lo, hi = pc.gs.lo[0].double(), pc.gs.hi[0].double()
-    pen = (((lo - Xr).clamp(min=0) ** 2 + (Xr - hi).clamp(min=0) ** 2).sum(-1) * lb64.heavy[:, None].double()).sum(-1) * 10.0
-    intra = p64.intra(Xr)
-    want_t = (inter + pen + intra).reshape(-1).numpy()
-    assert rel_close(et.cpu().numpy(), want_t, 1e-5, 1e-5) < 1e-5
-    assert rel_close(ei.cpu().numpy(), intra.reshape(-1).numpy(), 1e-5, 1e-5) < 1e-5
+    et, ei, X = kp.rescore64(torch.as_tensor(cl, device=dev), torch.as_tensor(st, device=dev), exact=exact)
+    want_t, want_i = _fp64_energies(pc, cl, st, exact)
+    assert rel_close(et.cpu().numpy(), want_t, 1e-7, 1e-7) < 1e-7
+    assert rel_close(ei.cpu().numpy(), want_i, 1e-7, 1e-7) < 1e-7
 
 
 @pytest.mark.parametrize("kind", ["mixed", "big"])
