@@ -58,6 +58,8 @@ _SIGS = {
     "adock_last_error": ([], ctypes.c_char_p),
     "adock_grid_vina": ([P, P, I, P, P, P, P, I, P, I, F, F, F, F, I, I, I, P, I, P, P], I),
     "adock_grid_fit": ([P, P, I, P, I, P, I, P, F, F, F, F, I, I, I, P, P, P], I),
+    "adock_grid_vina_cells": ([P, P, I, P, P, P, F, P, P, P, P, I, P, I, F, F, F, F, I, I, I, P, I, P, P], I),
+    "adock_grid_fit_cells": ([P, P, I, P, P, P, F, P, I, P, I, P, F, F, F, F, I, I, I, P, P, P], I),
     "adock_grid_convert": ([P, P, ctypes.c_longlong, I, P], I),
     "adock_prepare": ([SP(Ligands), SP(SF), SP(Work), P], I),
     "adock_eg": ([SP(Ligands), SP(Work), SP(Grids), SP(SF), SP(Receptors), P, I, P, P, P, I, P], I),

@@ -1,7 +1,7 @@
 """Receptor grid maps and their storage contract (reference ``src/adock/grid.py``, ``src/adock/fit/gridfit.py``).
 
 ``build_grid`` / ``build_grid_fit`` keep the reference signatures (grid.py:132, gridfit.py:71) and run the
-sm_100a kernels of ``libadock_b200.so``. ``GridSet`` keeps the reference storage contract (flat concatenation of
+sm_100a kernels of ``libadock_b200.so`` over a receptor cell list built here (``CellList``). ``GridSet`` keeps the reference storage contract (flat concatenation of
 per-receptor ``[T_r, nx, ny, nz]`` maps, ``offs``, ``dims``, ``slot``, ``origin``, ``lo``, ``hi``) and can carry an
 FP16/BF16 copy of ``flat`` for the search kernels (FP32 interpolation and accumulation either way).
 """
@@ -26,6 +26,32 @@ def _cuda_device(device):
     return dev
 
 
+CELL_MIN = 4.0   # A, edge of the receptor cell list's cells (at least)
+
+
+class CellList:
+    """Receptor atoms sorted by cell of a uniform grid (cubic cells of edge ``size`` from ``origin``), with the start
+    of every cell; cell (cx, cy, cz) = index (cx * ny + cy) * nz + cz. ``order`` is the sorting permutation (stable,
+    so atoms of one cell stay in receptor order)."""
+
+    def __init__(self, xyz, cutoff, spacing):
+        xyz = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
+        self.size = max(CELL_MIN, (4 * spacing + 2 * cutoff) / 7.0)
+        lo = xyz.min(0) if len(xyz) else np.zeros(3, np.float32)
+        hi = xyz.max(0) if len(xyz) else np.zeros(3, np.float32)
+        self.origin = (lo - 1e-3).astype(np.float32)
+        self.dims = np.maximum(np.ceil((hi - self.origin + 1e-3) / self.size).astype(np.int32), 1)
+        c = np.minimum(((xyz - self.origin) / self.size).astype(np.int64), self.dims - 1)
+        cid = (c[:, 0] * self.dims[1] + c[:, 1]) * self.dims[2] + c[:, 2]
+        self.order = np.argsort(cid, kind="stable")
+        self.start = np.concatenate([[0], np.cumsum(np.bincount(cid, minlength=int(self.dims.prod())))]).astype(np.int32)
+
+    def args(self, device):
+        """(start tensor on device, dims, origin, size) for the *_cells entry points."""
+        return (torch.as_tensor(self.start, device=device), np.ascontiguousarray(self.dims, np.int32),
+                np.ascontiguousarray(self.origin, np.float32), float(self.size))
+
+
 def build_grid(rec_xyz, rec_types, sfp, origin, spacing, n, lig_types=None, per_term=False, device="cuda"):
     """Return torch tensor [T, nx, ny, nz] (or [5, T, nx, ny, nz] unweighted if per_term) on ``device``.
 
@@ -37,15 +63,19 @@ def build_grid(rec_xyz, rec_types, sfp, origin, spacing, n, lig_types=None, per_
     lig_types = np.arange(T, dtype=np.int32) if lig_types is None else np.asarray(lig_types, dtype=np.int32)
     assert len(lig_types) <= MAX_TYPES
     dev = _cuda_device(device)
-    rx = torch.as_tensor(np.ascontiguousarray(rec_xyz, np.float32).reshape(-1, 3), device=dev)
-    rt = torch.as_tensor(np.ascontiguousarray(rec_types, np.int32), device=dev)
+    xyz = np.ascontiguousarray(rec_xyz, np.float32).reshape(-1, 3)
+    cells = CellList(xyz, float(sfp["cutoff"]), float(spacing))
+    rx = torch.as_tensor(xyz[cells.order], device=dev)
+    rt = torch.as_tensor(np.ascontiguousarray(np.asarray(rec_types)[cells.order], np.int32), device=dev)
+    cstart, cdims, corg, csize = cells.args(dev)
     nlt = len(lig_types)
     out = torch.empty(((5 if per_term else 1) * nlt * nx * ny * nz,), dtype=torch.float32, device=dev)
     tabs = [np.ascontiguousarray(sfp[k], np.int32) for k in ("hydrophobic", "donor", "acceptor")]
     rad = np.ascontiguousarray(sfp["radius"], np.float32)
     prm = grid_prm(sfp)
     with torch.cuda.device(dev):
-        _lib.call("adock_grid_vina", _lib.ptr(rx), _lib.ptr(rt), len(rx), _lib.ptr(rad), _lib.ptr(tabs[0]),
+        _lib.call("adock_grid_vina_cells", _lib.ptr(rx), _lib.ptr(rt), len(rx), _lib.ptr(cstart), _lib.ptr(cdims),
+                  _lib.ptr(corg), csize, _lib.ptr(rad), _lib.ptr(tabs[0]),
                   _lib.ptr(tabs[1]), _lib.ptr(tabs[2]), T, _lib.ptr(lig_types), nlt, float(origin[0]),
                   float(origin[1]), float(origin[2]), float(spacing), nx, ny, nz, _lib.ptr(prm), int(per_term),
                   _lib.ptr(out), _lib.stream_ptr())
@@ -62,15 +92,19 @@ def build_grid_fit(rec_xyz, rec_ext, pot, origin, spacing, n, device="cuda"):
         n = (int(n),) * 3
     nx, ny, nz = map(int, n)
     dev = _cuda_device(device)
-    rx = torch.as_tensor(np.ascontiguousarray(rec_xyz, np.float32).reshape(-1, 3), device=dev)
-    re = torch.as_tensor(np.ascontiguousarray(rec_ext, np.int32), device=dev)
+    xyz = np.ascontiguousarray(rec_xyz, np.float32).reshape(-1, 3)
+    cells = CellList(xyz, float(spec.cutoff), float(spacing))
+    rx = torch.as_tensor(xyz[cells.order], device=dev)
+    re = torch.as_tensor(np.ascontiguousarray(np.asarray(rec_ext)[cells.order], np.int32), device=dev)
+    cstart, cdims, corg, csize = cells.args(dev)
     W = torch.as_tensor(np.ascontiguousarray(np.asarray(pot.W, np.float32)), device=dev)
     rad_rec = torch.as_tensor(np.ascontiguousarray(spec.rec_radius, np.float32), device=dev)
     rad_lig = np.ascontiguousarray(pot.radius, np.float32)
     prm = spec.grid_prm()
     out = torch.empty((nlt * nx * ny * nz,), dtype=torch.float32, device=dev)
     with torch.cuda.device(dev):
-        _lib.call("adock_grid_fit", _lib.ptr(rx), _lib.ptr(re), len(rx), _lib.ptr(rad_rec), int(W.shape[0]),
+        _lib.call("adock_grid_fit_cells", _lib.ptr(rx), _lib.ptr(re), len(rx), _lib.ptr(cstart), _lib.ptr(cdims),
+                  _lib.ptr(corg), csize, _lib.ptr(rad_rec), int(W.shape[0]),
                   _lib.ptr(rad_lig), nlt, _lib.ptr(W), float(origin[0]), float(origin[1]), float(origin[2]),
                   float(spacing), nx, ny, nz, _lib.ptr(prm), _lib.ptr(out), _lib.stream_ptr())
     return out.view(nlt, nx, ny, nz)

@@ -265,7 +265,7 @@ def _best_per_ligand(best_e, L, M):
 
 def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(125, 250, 500, 1000, 2000),
                ref_steps=8000, train_steps=500, log_cap=2_000_000, epochs=3, learned=(("learned_f16", 32, 0.3),),
-               seed=0, log=None):
+               seed=0, log=None, learned_budgets=None, plain_f16=True):
     """Learned proposal vs plain MC at equal step budget (config-3 style evaluation).
 
     1. Training data: plain FP32 search (Stage-A starts, ``train_steps`` MC steps) on ``train_ligs`` with the
@@ -275,7 +275,9 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
        reported as the plain FP32 search's row at ``ref_steps``.
     3. For each budget S: plain FP32, plain FP16 and each learned FP16 variant (name, segment length prop_k,
        learned fraction prop_frac; proposals with plain fallback) from the same Stage-A starts;
-       gap(l) = E(l) - E_ref(l); reported: median and mean gap, ligands/s of Stage A + MC, evaluations per step.
+       gap(l) = E(l) - E_ref(l); reported: median and mean gap, ligands/s of Stage A + MC, evaluations per step
+       and per second. ``learned_budgets`` limits the learned variants' budgets; ``plain_f16=False`` skips the plain
+       FP16 rows.
     """
     dev = torch.device(device)
     from . import params
@@ -353,14 +355,16 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
                       cfg["mc_amp_pos"], cfg["mc_amp_rot"], seed + 3, 0)
         ev[1].record()
         torch.cuda.synchronize(dev)
+        ms = ev[0].elapsed_time(ev[1])
         st["evals_per_step"] = (int(kp.evals[0]) - ev0) / (cur.shape[0] * steps)
-        return _best_per_ligand(be, L, chains), ev[0].elapsed_time(ev[1]), st
+        st["evals_per_s"] = (int(kp.evals[0]) - ev0) / (ms / 1e3)
+        return _best_per_ligand(be, L, chains), ms, st
 
     ref, ref_ms, ref_st = run("plain_f32", ref_steps)
     results = {}
     out["learned_variants"] = {n: {"prop_k": k, "prop_frac": f, "target": t} for n, (k, f, t) in variants.items()}
-    for m in ("plain_f32", "plain_f16", *variants):
-        for S in budgets:
+    for m in ("plain_f32", *(("plain_f16",) if plain_f16 else ()), *variants):
+        for S in (learned_budgets or budgets if m in variants else budgets):
             results[(m, S)] = run(m, S)
     floor = ref.clone()
     for (e, _, _) in results.values():

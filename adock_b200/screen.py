@@ -1,9 +1,13 @@
-"""One pocket x many ligands with one shared grid set (reference ``src/adock/screen.py:39-78``).
+"""The callers of the search: one pocket x many ligands (``dock_screen``, reference ``src/adock/screen.py:39-78``)
+and many pockets x one ligand each (``dock_batch``, reference ``src/adock/dock.py:69-125``).
 
 ``dock_screen(receptor, box, ligands, ...)`` builds the receptor maps once on the GPU for the union of the
 ligands' types (plus C_H, the Stage-A probe type), then docks the ligands in batches against receptor 0 with
-``dock_problem_kernel``. Inputs are host data (receptor coordinates/types, ligand preps); results come back as
-host numpy arrays. This is the public call the end-to-end benchmark times.
+``dock_problem_kernel``. ``dock_batch(complexes, ...)`` takes prepared complexes (the reference's ``prepare_complex``
+output: receptor atoms, box and ligand prep), builds one map set per receptor with each complex's own ligand types,
+and docks every ligand against its own receptor and box in one search (receptor index = complex index). Inputs are
+host data; results come back as host numpy arrays. ``dock_screen`` is the public call the end-to-end benchmark
+times.
 """
 from __future__ import annotations
 
@@ -14,7 +18,7 @@ from . import params
 from .grid import make_gridset
 from .ligand import LigandBatch
 from .problem import PairPotential, Problem, pad_receptors
-from .search import dock_problem_kernel
+from .search import LAST_STATS, dock_problem, dock_problem_kernel
 
 
 def _nbytes(ts):
@@ -63,3 +67,45 @@ def dock_screen(receptor, box, ligands, cfg=None, device="cuda", seed=0, batch=N
         stats.update(st_all)
         stats["h2d_bytes"] = stats.get("h2d_bytes", 0) + int(h2d)
     return out
+
+
+def dock_batch(complexes, cfg=None, sf="vina", seed=0, device="cuda", log=None, timings=None, grid_dtype="f32"):
+    """complexes: dicts with rec_xyz [N, 3], rec_types [N], center [3], size [3] and lig (a ligand prep).
+
+    One search over all complexes: maps per receptor for its ligand's own types (plus the probe type), ligand l
+    docked against receptor l in box l. Returns one result dict per complex (coords trimmed to the ligand's atoms,
+    affinity, inter, intra, total, n_tors_vina); ``timings`` receives grid_s, search_s, n and the search
+    statistics (reference dock.py:113-125)."""
+    import time
+    cfg = dict(params.V2_DEFAULT if cfg is None else cfg)
+    dev = torch.device(device)
+    sfp = params.sf_params(sf)
+    recs = [{"rec_xyz": np.asarray(c["rec_xyz"], np.float32), "rec_types": np.asarray(c["rec_types"]),
+             "center": np.asarray(c["center"], float), "size": np.asarray(c["size"], float)} for c in complexes]
+    ligs = [c["lig"] for c in complexes]
+    t0 = time.perf_counter()
+    gs = make_gridset(recs, sfp, params.GRID_SPACING, params.OUT_OF_BOX_PENALTY, device=dev,
+                      lig_types=[np.asarray(l.types)[np.asarray(l.types) >= 0] for l in ligs])
+    prob = Problem(gs, LigandBatch(ligs, dev), torch.arange(len(ligs), device=dev), PairPotential(sfp, dev),
+                   rec=pad_receptors(recs, dev))
+    if dev.type == "cuda":
+        torch.cuda.synchronize(dev)
+    t1 = time.perf_counter()
+    bc = torch.tensor(np.array([r["center"] for r in recs]), dtype=torch.float32, device=dev)
+    kf = None
+    if grid_dtype != "f32":
+        from .kernel import B200KernelProblem
+        kf = lambda p: B200KernelProblem(p, grid_dtype=grid_dtype)
+    if kf is None:
+        res = dock_problem(prob, bc, [r["size"] for r in recs], cfg, seed=seed, log=log)
+    else:
+        LAST_STATS.clear()
+        res = dock_problem_kernel(prob, bc, [r["size"] for r in recs], cfg, seed=seed, log=log, stats=LAST_STATS,
+                                  kernel_factory=kf)
+    t2 = time.perf_counter()
+    if timings is not None:
+        timings.update({"grid_s": t1 - t0, "search_s": t2 - t1, "n": len(complexes), **LAST_STATS})
+    for lig, r in zip(ligs, res):
+        r["n_tors_vina"] = lig.n_tors_vina
+        r["coords"] = r["coords"][:, :lig.n]
+    return res

@@ -10,8 +10,9 @@ the data path (weak scaling).
 
 Prints one JSON line (rank 0). ``value`` times the search on device-resident inputs (maps, packed ligands);
 ``e2e`` times the public ``dock_screen`` call from host arrays (map build, packing, host<->device copies,
-search, results back on the host). ``--impl reference`` times the reference's own CPU kernels (oracle/_ref, the
-reference's g++/OpenMP build) driven by the same search driver on the host cores, on a 4-ligand sample.
+search, results back on the host). ``--impl reference`` times the reference's own search, unmodified (its driver
+``search.dock_problem_kernel`` with device "cpu" and its g++/OpenMP kernels, installed under baseline/_ref), on the
+host cores, on a 4-ligand sample.
 """
 import argparse
 import json
@@ -46,6 +47,11 @@ def _args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the map-builder / map-precision section")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="skip the learned-proposal section (FP16 maps + learned proposal vs plain FP32 at equal "
+                         "median gap, screening shapes, reduced ligand counts)")
+    ap.add_argument("--learned-train", type=int, default=512, help="training ligands of the learned-proposal section")
+    ap.add_argument("--learned-eval", type=int, default=256, help="held-out ligands of the learned-proposal section")
     ap.add_argument("--ab", action="store_true", help="learned proposal vs plain MC at equal step budget")
     ap.add_argument("--ab-train", type=int, default=256, help="fresh ligands for the proposal's training data")
     ap.add_argument("--ab-eval", type=int, default=256, help="held-out ligands for the A/B comparison")
@@ -150,65 +156,79 @@ def _traffic_per_atom_eval():
     return _profile_figure("dram_bytes_per_atom_eval")
 
 
+REF_INSTALL = ROOT / "baseline" / "_ref"
+
+
+def _stock_reference():
+    """The reference package installed unmodified under baseline/_ref (pip install --target), imported
+    with empty stand-ins for cupy and rdkit, which its CPU path does not use. Its CPU kernels are compiled on first
+    use by its own adock.cpukernel (g++ -O3 -march=native -ffast-math -fopenmp, all host threads) into a temporary
+    cache. Returns the modules, or None when the install is absent."""
+    if not (REF_INSTALL / "adock" / "search.py").exists():
+        return None
+    import tempfile
+    import types
+    for name in ("cupy", "rdkit", "rdkit.Chem"):
+        sys.modules.setdefault(name, types.ModuleType(name))
+    sys.modules["rdkit"].Chem = sys.modules["rdkit.Chem"]
+    os.environ.setdefault("ADOCK_CPU_CACHE", tempfile.mkdtemp(prefix="adock_ref_cpu_"))
+    os.environ.setdefault("ADOCK_CPU_THREADS", str(len(os.sched_getaffinity(0))))
+    if str(REF_INSTALL) not in sys.path:
+        sys.path.insert(0, str(REF_INSTALL))
+    from adock import grid, ligand, scoring, search
+    return types.SimpleNamespace(grid=grid, ligand=ligand, scoring=scoring, search=search,
+                                 threads=int(os.environ["ADOCK_CPU_THREADS"]))
+
+
+def _reference_problem(A, rec, ligs):
+    """The reference's Problem for a ligand list: its make_gridset (its CPU grid kernel), LigandBatch, Problem and
+    receptor padding, unchanged; built once per sample, outside the timed searches (its screening caller shares one
+    map set across all ligands, screen.py:55-56)."""
+    import numpy as np
+    import torch
+    from adock_b200 import params
+    sfp = params.sf_params("vina")          # the same constants as the reference's config/adock.json "scoring"
+    lt = np.unique(np.concatenate([[0]] + [l.types for l in ligs]))
+    gs = A.grid.make_gridset([rec], sfp, params.GRID_SPACING, params.OUT_OF_BOX_PENALTY, device="cpu", lig_types=[lt])
+    prob = A.search.Problem(gs, A.ligand.LigandBatch(ligs, "cpu"), torch.zeros(len(ligs), dtype=torch.long),
+                            A.scoring.PairPotential(sfp), rec=A.search.pad_receptors([rec], "cpu"))
+    prob._box = (torch.tensor(rec["center"], dtype=torch.float32)[None].expand(len(ligs), 3), [rec["size"]] * len(ligs))
+    return prob
+
+
+def _reference_search(A, prob, cfg, seed=0):
+    """One stock reference search (dock_problem_kernel with device "cpu") on the host cores: (seconds, results)."""
+    t0 = time.perf_counter()
+    res = A.search.dock_problem_kernel(prob, *prob._box, cfg, seed=seed)
+    return time.perf_counter() - t0, res
+
+
 def run_reference(args, rank, world):
-    """Reference arm: the reference's CPU kernels (oracle/_ref) on the host cores, 4-ligand sample per step."""
+    """Reference arm: the reference's own search (its driver, Stage A, CPU kernels, finalize; unmodified) on the host
+    cores, one 4-ligand sample of the workload per step."""
     if rank != 0:
         return None
     import torch
-    from oracle import ref as R
-    from adock_b200.search import dock_problem_kernel
-    if not R.available():
-        return {"impl": "reference", "unavailable": "oracle/_ref (the reference's CPU build) was not built on this tree"}
-    threads = R.threads()
-    torch.set_num_threads(threads)
+    A = _stock_reference()
+    if A is None:
+        return {"impl": "reference", "unavailable": "the reference package is not installed under baseline/_ref"}
+    torch.set_num_threads(A.threads)
     rec, ligs, cfg = _workload(0, args.ligands, args.mc_steps)
     sample = _cpu_sample(ligs)
-    prob = _cpu_problem(rec, sample)
-    # warm-up steps load the libraries and page in the inputs; they run a 20-step budget (untimed)
-    for _ in range(args.warmup):
-        dock_problem_kernel(prob, prob._bc, prob._bs, dict(cfg, mc_steps=20, mc_segment=20), seed=0,
-                            kernel_factory=R.RefKernelProblem)
-    times = []
-    for it in range(args.steps):
-        t0 = time.perf_counter()
-        dock_problem_kernel(prob, prob._bc, prob._bs, cfg, seed=0, kernel_factory=R.RefKernelProblem)
-        times.append(time.perf_counter() - t0)
+    prob = _reference_problem(A, rec, sample)
+    for _ in range(args.warmup):      # compiles the reference's kernels, pages in the inputs (20-step budget, untimed)
+        _reference_search(A, prob, dict(cfg, mc_steps=20, mc_segment=20))
+    times = [_reference_search(A, prob, cfg)[0] for _ in range(args.steps)]
     v = len(sample) * len(times) / sum(times)
     sample_desc = (f"{len(sample)} ligands of the workload (heavy atoms {[p.n for p in sample]}) x {CHAINS} chains x "
-                   f"{args.mc_steps} steps, full search per step")
+                   f"{args.mc_steps} steps, the full stock search per step (maps built once, untimed)")
     return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "impl": "reference",
             "config": {"workload": WORKLOAD, "ligands_per_step": len(sample), "chains": CHAINS, "mc_steps": args.mc_steps,
                        "parallelism": "host cores (OpenMP)"},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample_desc},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": A.threads, "kind": "reference", "sample": sample_desc},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-
-
-def _cpu_problem(rec, ligs):
-    """Problem on the host for the CPU baselines: maps from the reference CPU builder."""
-    import numpy as np
-    import torch
-    from oracle import ref as R
-    from adock_b200 import params
-    from adock_b200.grid import GridSet, grid_dims
-    from adock_b200.ligand import LigandBatch
-    from adock_b200.problem import PairPotential, Problem, pad_receptors
-    sfp = params.sf_params("vina")
-    lt = np.unique(np.concatenate([[0]] + [l.types for l in ligs]))
-    c, s = rec["center"], rec["size"]
-    o = c - s / 2
-    G = R.build_grid(rec["rec_xyz"], rec["rec_types"], sfp, o, params.GRID_SPACING, grid_dims(s, params.GRID_SPACING), lt)
-    slot = -np.ones((1, params.N_XS), np.int64)
-    slot[0, lt] = np.arange(len(lt))
-    f = lambda a: torch.tensor(np.asarray(a, np.float32)[None])
-    gs = GridSet([torch.as_tensor(G)], f(o), f(o), f(c + s / 2), params.GRID_SPACING, params.OUT_OF_BOX_PENALTY,
-                 slot=torch.as_tensor(slot), n_types=params.N_XS)
-    lb = LigandBatch(ligs, "cpu")
-    prob = Problem(gs, lb, torch.zeros(len(ligs), dtype=torch.long), PairPotential(sfp), rec=pad_receptors([rec], "cpu"))
-    prob._bc = torch.tensor(c, dtype=torch.float32)[None].expand(len(ligs), 3)
-    prob._bs = [s] * len(ligs)
-    return prob
 
 
 def run_ours(args, rank, world, local_rank):
@@ -355,9 +375,52 @@ def run_ours(args, rank, world, local_rank):
         out["screening"] = ab_compare(rec2, train, held, device=dev, budgets=(250, 500, 1000, 2000, 4000),
                                       learned=parse_variants(args.screen_variants), log_cap=args.screen_log_cap)
         out["screening"]["wall_s"] = time.perf_counter() - t0
+    if rank == 0 and world == 1 and not args.no_learned:
+        out["learned_proposal"] = _learned_section(dev, args.learned_train, args.learned_eval)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = _cpu_baseline(ligs, rec, cfg)
     return out
+
+
+def _learned_section(dev, n_train, n_eval):
+    """The learned half of the metric on the screening shapes (the 8,000-atom receptor, 30 A box, 81^3 x 8 maps;
+    ligands with 8-80 heavy atoms and 0-20 torsions), at reduced ligand counts: the proposal network is trained on
+    the plain search's own moves from n_train fresh ligands (two self-training rounds, <= 2 M logged moves per
+    collection), then FP16 maps + learned proposal and plain FP32 dock n_eval held-out ligands x 32 chains from
+    the same Stage-A starts at several step budgets. Gap = a ligand's best energy minus the lowest energy any run
+    found for it (an 8,000-step plain run included). Reported: ligands/s and energy evaluations/s of each method
+    at the budget where its median gap reaches 0.1 kcal/mol (interpolated between budgets), and their ratio."""
+    from adock_b200 import synth
+    from adock_b200.proposal import ab_compare
+    rec2 = synth.config_receptor(2)
+    train = synth.ligand_set(n_train, (8, 80), (0, 20), seed0=300_000)
+    held = synth.ligand_set(n_eval, (8, 80), (0, 20), seed0=400_000)
+    t0 = time.perf_counter()
+    ab = ab_compare(rec2, train, held, device=dev, budgets=(250, 500, 1000, 2000, 4000),
+                    learned=[("learned_f16", 32, 0.3, "dagger2")], log_cap=2_000_000,
+                    learned_budgets=(250, 500, 1000, 2000), plain_f16=False)
+    wall = time.perf_counter() - t0
+    interp = ab.get("interp_at_gap_0.1", {})
+
+    def at_bar(m):
+        r = interp.get(m)
+        if not r:
+            return None
+        rows = sorted(ab["methods"][m], key=lambda x: x["steps"])
+        near = min(rows, key=lambda x: abs(x["steps"] - r["steps"]))
+        return {"steps": r["steps"], "ligands_per_s": r["ligands_per_s"], "evals_per_s": near["evals_per_s"]}
+
+    plain, learned = at_bar("plain_f32"), at_bar("learned_f16")
+    return {"workload": (f"screening shapes: 8000-atom receptor, 30 A box, 81^3 x 8 maps; {n_eval} held-out ligands "
+                         f"(8-80 heavy atoms, 0-20 torsions) x 32 chains; proposal trained on {n_train} fresh "
+                         f"ligands (2 self-training rounds)"),
+            "gap_bar_kcal_mol": 0.1, "plain_f32": plain, "learned_f16": learned,
+            "speedup_ligands_per_s_at_gap_0.1": (learned["ligands_per_s"] / plain["ligands_per_s"]
+                                                 if plain and learned else None),
+            "train_ms": {k: v["train_ms"] for k, v in ab["train"].items() if isinstance(v, dict)},
+            "train_moves": ab["train"]["moves"], "wall_s": wall,
+            "rows": {m: [{k: r[k] for k in ("steps", "median_gap", "mean_gap", "ligands_per_s", "evals_per_s")}
+                         for r in rs] for m, rs in ab["methods"].items()}}
 
 
 def _grid_and_precision(dev, ligs):
@@ -404,25 +467,21 @@ def _grid_and_precision(dev, ligs):
 
 
 def _cpu_baseline(ligs, rec, cfg):
-    """The reference CPU kernels (or the oracle's restatement where oracle/_ref is absent) on a 4-ligand sample."""
+    """The reference's own search (stock driver and CPU kernels, baseline/_ref) on the host cores, on a 4-ligand
+    quantile sample of the workload."""
     import torch
-    from oracle import port
-    from oracle import ref as R
-    from adock_b200.search import dock_problem_kernel
+    A = _stock_reference()
     sample = _cpu_sample(ligs)
-    threads = R.threads()
-    torch.set_num_threads(threads)
-    prob = _cpu_problem(rec, sample) if R.available() else None
-    kind = "reference" if R.available() else "port"
-    if prob is None:
-        return {"value": None, "unit": UNIT, "cores": threads, "kind": kind, "sample": "oracle/_ref not built"}
-    factory = R.RefKernelProblem if kind == "reference" else (lambda p: R.RefKernelProblem(p, port.PortProblem))
-    t0 = time.perf_counter()
-    dock_problem_kernel(prob, prob._bc, prob._bs, cfg, seed=0, kernel_factory=factory)
-    dt = time.perf_counter() - t0
-    return {"value": len(sample) / dt, "unit": UNIT, "cores": threads, "kind": kind,
+    if A is None:
+        return {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
+                "sample": "unavailable: the reference package is not installed under baseline/_ref"}
+    torch.set_num_threads(A.threads)
+    prob = _reference_problem(A, rec, sample)
+    _reference_search(A, prob, dict(cfg, mc_steps=20, mc_segment=20))     # compile + page in (untimed)
+    dt, _ = _reference_search(A, prob, cfg)
+    return {"value": len(sample) / dt, "unit": UNIT, "cores": A.threads, "kind": "reference",
             "sample": f"{len(sample)} ligands (heavy atoms {[p.n for p in sample]}) x {CHAINS} chains x "
-                      f"{cfg['mc_steps']} steps, one full search, {dt:.1f} s"}
+                      f"{cfg['mc_steps']} steps, one full stock search, {dt:.1f} s"}
 
 
 def main():

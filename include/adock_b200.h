@@ -157,6 +157,22 @@ int adock_grid_fit(const float* rec_xyz, const int* rec_ext, int n_rec, const fl
                    const float* rad_lig, int n_lt, const float* W, float ox, float oy, float oz, float spacing,
                    int nx, int ny, int nz, const float* prm, float* out, void* stream);
 
+/* The same two builders over a receptor cell list: rec_xyz / rec_types (or rec_ext) sorted by cell of a uniform
+ * grid of cubic cells of edge cell_size from cell_origin [3] (host), cell_dims [3] cells per axis (host), and
+ * cell_start [nx*ny*nz + 1] (dev): cell (cx, cy, cz) holds atoms [cell_start[c], cell_start[c+1]) with
+ * c = (cx * ny + cy) * nz + cz. A tile of grid points reads only the cells within the cutoff of it (at most 8 x 8
+ * columns of cells: cell_size >= (4 * spacing + 2 * cutoff) / 7); atoms outside the cell grid are not seen.
+ * No reference counterpart (an input layout of the same kernels). */
+int adock_grid_vina_cells(const float* rec_xyz, const int* rec_types, int n_rec, const int* cell_start,
+                          const int* cell_dims, const float* cell_origin, float cell_size, const float* radius,
+                          const int* hyd, const int* don, const int* acc, int n_xs, const int* lig_types, int n_lt,
+                          float ox, float oy, float oz, float spacing, int nx, int ny, int nz, const float* prm,
+                          int per_term, float* out, void* stream);
+int adock_grid_fit_cells(const float* rec_xyz, const int* rec_ext, int n_rec, const int* cell_start,
+                         const int* cell_dims, const float* cell_origin, float cell_size, const float* rad_rec, int n_rt,
+                         const float* rad_lig, int n_lt, const float* W, float ox, float oy, float oz, float spacing,
+                         int nx, int ny, int nz, const float* prm, float* out, void* stream);
+
 /* Down-convert FP32 maps to FP16 (dtype ADOCK_GRID_F16, saturating at +-65504) or BF16 (ADOCK_GRID_BF16), round
  * to nearest. No reference counterpart (the reference stores FP32 maps only). */
 int adock_grid_convert(const float* src, void* dst, long long n, int dtype, void* stream);

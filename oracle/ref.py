@@ -193,87 +193,3 @@ def build_grid_fit(rec_xyz, rec_ext, W, rad_rec, rad_lig, prm12, origin, spacing
     fit_lib().launch_build_grid_fit(_p(rx), _p(re), len(rx), _p(rr), _p(rl), TL, _p(W), float(origin[0]),
                                     float(origin[1]), float(origin[2]), float(spacing), nx, ny, nz, _p(pr), _p(out))
     return out.reshape(TL, nx, ny, nz)
-
-
-class RefKernelProblem:
-    """Torch-CPU front end of the reference CPU kernels with the reference ``CpuKernelProblem`` interface
-    (``src/adock/cpukernel.py:231-306``): same packing, state layout and methods, so the reference's search
-    driver structure (``search.py:544-671``) runs on it unchanged. Neighbour lists follow
-    ``mckernel.py:662-688`` (torch cdist)."""
-
-    def __init__(self, prob, backend=None):
-        """backend: RefProblem (default, the reference's CPU build) or oracle.port.PortProblem (restatement)."""
-        import torch
-        from adock_b200.problem import pack_host
-        self.AM, self.KM, lig, sf = pack_host(prob)
-        gs = prob.gs
-        grid = dict(flat=gs.flat.float().cpu().numpy(), origin=gs.origin.cpu().numpy(), lo=gs.lo.cpu().numpy(),
-                    hi=gs.hi.cpu().numpy(), rec_idx=prob.rec_idx.cpu().numpy(), offs=gs.offs.cpu().numpy(),
-                    dims=gs.dims.cpu().numpy(), T=gs.T, spacing=gs.spacing, penalty=gs.penalty)
-        rec = None
-        if prob.rec is not None:
-            rx, rt, rm = prob.rec
-            rec = (rx.cpu().numpy(), rt.cpu().numpy(), rm.sum(1).cpu().numpy())
-        self.rp = (backend or RefProblem)(self.AM, self.KM, lig, sf, grid, rec)
-        self.L, self.SD, self.DM = prob.lb.L, 7 + self.KM, 6 + self.KM
-        self._torch = torch
-
-    def pack(self, t, q, theta):
-        torch = self._torch
-        N, K = theta.shape
-        s = torch.zeros(N, self.SD, dtype=torch.float32)
-        s[:, :3], s[:, 3:7] = t, q
-        s[:, 7:7 + min(K, self.KM)] = theta[:, :self.KM]
-        return s.contiguous()
-
-    def unpack(self, s, K):
-        import math
-        torch = self._torch
-        th = torch.zeros(s.shape[0], K, dtype=s.dtype)
-        th[:, :min(K, self.KM)] = s[:, 7:7 + min(K, self.KM)]
-        th = torch.remainder(th + math.pi, 2 * math.pi) - math.pi
-        return s[:, :3].clone(), s[:, 3:7] / s[:, 3:7].norm(dim=-1, keepdim=True), th
-
-    def energy_grad(self, chain_lig, state, exact=False):
-        torch = self._torch
-        e, g = self.rp.energy_grad(chain_lig.numpy(), state.float().contiguous().numpy(), exact)
-        return torch.from_numpy(e), torch.from_numpy(g)
-
-    def stage_a(self, conf_h, quats, trans, ntrans, cap):
-        torch = self._torch
-        be, bi = self.rp.stage_a(conf_h.float().contiguous().numpy(), quats.float().contiguous().numpy(),
-                                 trans.float().contiguous().numpy(), ntrans.numpy(), cap)
-        return torch.from_numpy(be), torch.from_numpy(bi)
-
-    def run_mc(self, chain_lig, chain_id, cur, cur_e, best, best_e, init_opt, mc_steps, bfgs_iters, temp,
-               amp_pos, amp_rot, seed, step_offset, exact=False, nbr=None, nbr_n=None):
-        self.rp.run_mc(chain_lig.numpy(), chain_id.numpy(), cur.numpy(), cur_e.numpy(), best.numpy(), best_e.numpy(),
-                       init_opt, mc_steps, bfgs_iters, temp, amp_pos, amp_rot, seed, step_offset, exact,
-                       None if nbr is None else nbr.numpy(), None if nbr_n is None else nbr_n.numpy())
-
-    def receptor_neighbours(self, prob, chain_lig, states, K, margin):
-        """Per chain: receptor atoms within cutoff + margin of any heavy atom of the pose, in receptor order."""
-        import numpy as np
-        from adock_b200.problem import pack_host
-        from oracle.fp64 import Packed
-        torch = self._torch
-        rx, rt, rm = prob.rec
-        cut = float(prob.pot.p["cutoff"]) + margin
-        AM, KM, lig, sf = pack_host(prob)
-        model = Packed(lig, sf)
-        st = states.double().numpy()
-        cl = chain_lig.long().numpy()
-        near_all = []
-        for n in range(len(st)):
-            l = int(cl[n])
-            X = model.pose_heavy(l, st[n:n + 1])[0]
-            ri = int(prob.rec_idx[l])
-            xr = rx[ri][rm[ri]].double().numpy()
-            near_all.append(np.flatnonzero((np.linalg.norm(X[:, None] - xr[None], axis=-1) < cut).any(0)))
-        NB = max(1, max(len(x) for x in near_all))
-        nbr = torch.zeros(len(st), NB, dtype=torch.int32)
-        nbr_n = torch.zeros(len(st), dtype=torch.int32)
-        for n, near in enumerate(near_all):
-            nbr[n, :len(near)] = torch.as_tensor(near, dtype=torch.int32)
-            nbr_n[n] = len(near)
-        return nbr, nbr_n

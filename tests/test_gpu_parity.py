@@ -57,6 +57,29 @@ def test_grid_per_term_and_ragged(dev):
         assert rel_close(gg, gc, 1e-5) < 1e-5
 
 
+def test_grid_cell_list_matches_whole_receptor_scan(dev):
+    """build_grid (receptor cell list, adock_grid_vina_cells) against adock_grid_vina (every CTA scans the whole
+    receptor in receptor order): the same maps up to the summation order (rel 1e-6)."""
+    from adock_b200 import _lib, params
+    from adock_b200.grid import build_grid, grid_dims
+    sfp = params.sf_params("vina")
+    rec = receptor("cfg0")
+    lt = np.array([0, 2, 3, 4, 8, 9, 10, 17], np.int32)
+    o = rec["center"] - rec["size"] / 2
+    n = grid_dims(rec["size"], SPACING)
+    G = build_grid(rec["rec_xyz"], rec["rec_types"], sfp, o, SPACING, n, lt, device=dev)
+    rx = torch.as_tensor(np.asarray(rec["rec_xyz"], np.float32), device=dev)
+    rt = torch.as_tensor(np.asarray(rec["rec_types"], np.int32), device=dev)
+    out = torch.empty(len(lt) * int(np.prod(n)), device=dev)
+    tabs = [np.ascontiguousarray(sfp[k], np.int32) for k in ("hydrophobic", "donor", "acceptor")]
+    rad = np.ascontiguousarray(sfp["radius"], np.float32)
+    prm = params.grid_prm(sfp)
+    _lib.call("adock_grid_vina", _lib.ptr(rx), _lib.ptr(rt), len(rx), _lib.ptr(rad), _lib.ptr(tabs[0]), _lib.ptr(tabs[1]),
+              _lib.ptr(tabs[2]), len(rad), _lib.ptr(lt), len(lt), float(o[0]), float(o[1]), float(o[2]), SPACING,
+              int(n[0]), int(n[1]), int(n[2]), _lib.ptr(prm), 0, _lib.ptr(out), _lib.stream_ptr())
+    assert rel_close(G.cpu().numpy().reshape(-1), out.cpu().numpy(), 1e-6) < 1e-6
+
+
 def test_grid_fit_matches_oracle(dev):
     _need_oracle()
     from adock_b200 import params
