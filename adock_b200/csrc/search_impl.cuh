@@ -25,6 +25,7 @@ namespace adock {
 #define ADOCK_COLD_ATTR __forceinline__
 #endif
 #define PAIR_ROUNDS_MAX 256   // pair schedule: at most 256 rounds of 32 (8,192 pairs) are reordered
+#define PAIR_QUEUE 64         // per-warp ring of intra pairs found inside the cutoff, evaluated 32 at a time
 
 struct SearchParams {
     // B200 working layout
@@ -111,12 +112,14 @@ __device__ __forceinline__ void stage_tables(TypeTables& dst, const TypeTables& 
 // ------------------------------------------------------------------------------------------ per-warp workspace
 // Float offsets of the per-warp shared workspace for a given AM / KM (float4 arrays first).
 struct WSLayout {
-    int X, FF, ap, au, tp, tu, mk, ax, cs, sn, H, x, xn, xo, cur, best, g, gn, go, p, y, mhy, total;
+    int X, FF, qd, qr, ap, au, tp, tu, mk, ax, cs, sn, H, x, xn, xo, cur, best, g, gn, go, p, y, mhy, total;
     __host__ __device__ WSLayout(int AM, int KM) {
         const int DM = 6 + KM, SD = 7 + KM;
         int o = 0;
         X = o; o += 3 * AM;    // world coordinates, [3][AM] (x, y, z arrays)
         FF = o; o += 3 * AM;   // forces, [3][AM]
+        qd = o; o += 4 * PAIR_QUEUE;   // in-cutoff pair queue: separation (x, y, z) and r^2 (float4)
+        qr = o; o += 2 * PAIR_QUEUE;   // in-cutoff pair queue: pair record (int2)
         ap = o; o += 4 * KM;
         au = o; o += 4 * KM;
         tp = o; o += 4 * KM;
@@ -246,24 +249,22 @@ __device__ __forceinline__ float trilinear(const GT* G, int ny, int nz, const fl
     return e;
 }
 
-// Intra-ligand pair term of one scheduled slot: energy, and the force added into both atoms' entries. Positions X
-// and forces F are three arrays of AM floats each (x, y, z), so that 32 lanes touching 32 different atoms hit 32
-// different shared-memory banks (a float4 per atom would put the x components of 32 atoms on 8 banks).
+// Intra-ligand pair term of one queued pair (record pr, separation d.xyz = X_i - X_j, d.w = r^2): energy, and the
+// force added into both atoms' entries. Positions and forces are three arrays of AM floats each (x, y, z), so that
+// 32 lanes touching 32 different atoms hit 32 different shared-memory banks (a float4 per atom would put the x
+// components of 32 atoms on 8 banks).
 template <int AM>
-__device__ __forceinline__ float pair_slot(int2 pr, const float* X, float* F, const PairPrm& pp) {
-    if (pr.x < 0) return 0.f;
+__device__ __forceinline__ float pair_eval(int2 pr, float4 d, float* F, const PairPrm& pp) {
     const int i = pr.x & 0xff, j = (pr.x >> 8) & 0xff, fl = pr.x >> 16;
-    const float rx = X[i] - X[j], ry = X[AM + i] - X[AM + j], rz = X[2 * AM + i] - X[2 * AM + j];
     // r and 1/r from one reciprocal square root; clamping r^2 at 1e-12 is the reference's max(r, 1e-6)
-    const float r2 = rx * rx + ry * ry + rz * rz;
-    const float rinv = rsqrtf(fmaxf(r2, 1e-12f));
-    const float r = r2 * rinv;
+    const float rinv = rsqrtf(fmaxf(d.w, 1e-12f));
+    const float r = d.w * rinv;
     if (r >= pp.cutoff) return 0.f;
     float de;
     const float e = pair_energy(r, __int_as_float(pr.y), fl, pp, de);
     const float sc = de * rinv;
-    atomicAdd(F + i, sc * rx); atomicAdd(F + AM + i, sc * ry); atomicAdd(F + 2 * AM + i, sc * rz);
-    atomicAdd(F + j, -sc * rx); atomicAdd(F + AM + j, -sc * ry); atomicAdd(F + 2 * AM + j, -sc * rz);
+    atomicAdd(F + i, sc * d.x); atomicAdd(F + AM + i, sc * d.y); atomicAdd(F + 2 * AM + i, sc * d.z);
+    atomicAdd(F + j, -sc * d.x); atomicAdd(F + AM + j, -sc * d.y); atomicAdd(F + 2 * AM + j, -sc * d.z);
     return e;
 }
 
@@ -368,20 +369,52 @@ __device__ __forceinline__ float eval_eg(float* ws, const WSLayout& L, const flo
         }
     }
     __syncwarp();
-    // intra-ligand pairs, scheduled in rounds of 32 in which an atom appears at most once (adock_prepare), so the
-    // force atomics of one round do not collide; two rounds in flight per iteration
-    // the next two rounds' records are loaded while the current two are evaluated
+    // intra-ligand pairs, in two stages. Stage 1 walks the scheduled rounds of 32 (adock_prepare: an atom appears at
+    // most once per round where possible) and computes each pair's separation; the pairs inside the cutoff (about
+    // half of them: the rest contribute nothing) are appended to a per-warp ring by ballot. Stage 2 evaluates the
+    // terms and force atomics of 32 queued pairs whenever the ring holds that many, so its lanes are all busy.
+    // Records of the next two rounds are loaded ahead.
     {
+        float4* qd = (float4*)(ws + L.qd);
+        int2* qr = (int2*)(ws + L.qr);
+        const float keep2 = P.pp.cutoff * P.pp.cutoff * 1.0001f;   // stage 1 keeps a margin; stage 2 tests r < cutoff
+        const unsigned below = (1u << lane) - 1u;
         const int2 none = make_int2(-1, 0);
         int2 pa = c.nrounds > 0 ? c.pairs[lane] : none;
         int2 pb = c.nrounds > 1 ? c.pairs[32 + lane] : none;
-        for (int r = 0; r < c.nrounds; r += 2) {
-            const int2 qa = (r + 2 < c.nrounds) ? c.pairs[(r + 2) * 32 + lane] : none;
-            const int2 qb = (r + 3 < c.nrounds) ? c.pairs[(r + 3) * 32 + lane] : none;
-            e += pair_slot<AM>(pa, X, FF, P.pp);
-            e += pair_slot<AM>(pb, X, FF, P.pp);
-            pa = qa;
-            pb = qb;
+        int head = 0, fill = 0;
+        for (int r = 0; r < c.nrounds; ++r) {
+            const int2 pr = pa;
+            pa = pb;
+            pb = (r + 2 < c.nrounds) ? c.pairs[(r + 2) * 32 + lane] : none;
+            bool keep = false;
+            float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (pr.x >= 0) {
+                const int i = pr.x & 0xff, j = (pr.x >> 8) & 0xff;
+                d.x = X[i] - X[j]; d.y = X[AM + i] - X[AM + j]; d.z = X[2 * AM + i] - X[2 * AM + j];
+                d.w = d.x * d.x + d.y * d.y + d.z * d.z;
+                keep = d.w < keep2;
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, keep);
+            if (keep) {
+                const int q = (head + fill + __popc(bal & below)) & (PAIR_QUEUE - 1);
+                qd[q] = d;
+                qr[q] = pr;
+            }
+            fill += __popc(bal);
+            if (fill >= 32) {
+                __syncwarp();
+                const int q = (head + lane) & (PAIR_QUEUE - 1);
+                e += pair_eval<AM>(qr[q], qd[q], FF, P.pp);
+                head = (head + 32) & (PAIR_QUEUE - 1);
+                fill -= 32;
+                __syncwarp();   // the ring slots just read may be refilled by the next round
+            }
+        }
+        __syncwarp();
+        if (lane < fill) {
+            const int q = (head + lane) & (PAIR_QUEUE - 1);
+            e += pair_eval<AM>(qr[q], qd[q], FF, P.pp);
         }
     }
     // world torsion axes (axis atoms' current positions)
