@@ -110,80 +110,29 @@ def build_grid_fit(rec_xyz, rec_ext, pot, origin, spacing, n, device="cuda"):
     return out.view(nlt, nx, ny, nz)
 
 
-def trilinear(flat, origin, lo, hi, x, t, rec_idx, mask, dims, offs, slot, spacing: float, penalty: float):
-    """Torch trilinear lookup + quadratic out-of-box penalty (grid.py:169-194); differentiable w.r.t. x."""
-    o = origin[rec_idx]
-    dm = dims[rec_idx]
-    f = (x - o) / spacing
-    fc = torch.minimum(f.clamp(min=0.0), (dm - 1).to(f.dtype) - 1e-4)
-    i0 = fc.detach().floor().long()
-    w = fc - i0
-    ny, nz = dm[..., 1], dm[..., 2]
-    base = offs[rec_idx] + slot[rec_idx, t.clamp(min=0)].clamp(min=0) * (dm[..., 0] * ny * nz)
-    e = 0.0
-    for dx in (0, 1):
-        wx = w[..., 0] if dx else 1 - w[..., 0]
-        for dy in (0, 1):
-            wy = w[..., 1] if dy else 1 - w[..., 1]
-            for dz in (0, 1):
-                wz = w[..., 2] if dz else 1 - w[..., 2]
-                idx = base + ((i0[..., 0] + dx) * ny + (i0[..., 1] + dy)) * nz + (i0[..., 2] + dz)
-                e = e + wx * wy * wz * flat[idx].to(wx.dtype)
-    out = (lo[rec_idx] - x).clamp(min=0) ** 2 + (x - hi[rec_idx]).clamp(min=0) ** 2
-    e = e + penalty * out.sum(-1)
-    if mask is not None:
-        e = torch.where(mask, e, torch.zeros_like(e))
-    return e
-
-
 class GridSet:
-    """Batch of receptor grids with per-receptor origin and box (grid.py:197-248).
-
-    grids: stacked tensor [R, T, n, n, n] (common cube) or a list of per-receptor tensors [T, nx, ny, nz].
-    slot: optional [R, n_types] (global type -> grid slot, -1 = not built); default identity."""
+    """Maps of R receptors in the reference's storage contract (``grid.py:197-248``): ``flat`` concatenates every
+    receptor's ``[T_r, nx, ny, nz]`` block (z fastest), with ``offs`` [R] element offsets, ``dims`` [R, 3], ``slot``
+    [R, n_types] (global XS type -> map index, -1 = not built), ``origin``, ``lo``, ``hi`` [R, 3], ``spacing`` and
+    ``penalty``. ``grids`` is either a stacked tensor [R, T, n, n, n] (a common cube, kept as ``G``) or a list of
+    per-receptor tensors. Without ``slot`` every receptor holds all T types in order."""
 
     def __init__(self, grids, origins, box_lo, box_hi, spacing, penalty, slot=None, n_types=None):
         dev = origins.device
-        if torch.is_tensor(grids):
-            self.G = grids
-            self.R, self.T, self.n = grids.shape[0], grids.shape[1], grids.shape[2]
-            self.flat = grids.reshape(-1)
-            sz = self.T * self.n ** 3
-            self.dims = torch.full((self.R, 3), self.n, dtype=torch.long, device=dev)
-            self.offs = torch.arange(self.R, device=dev, dtype=torch.long) * sz
-        else:
-            self.G = None
-            self.R, self.T = len(grids), grids[0].shape[0]
-            self.flat = torch.cat([g.reshape(-1) for g in grids])
-            self.dims = torch.tensor([list(g.shape[1:]) for g in grids], dtype=torch.long, device=dev)
-            sizes = torch.tensor([g.numel() for g in grids], dtype=torch.long, device=dev)
-            self.offs = torch.cumsum(sizes, 0) - sizes
-            self.n = int(self.dims.max())
-        if slot is None:
-            slot = torch.arange(self.T, device=dev).expand(self.R, self.T).contiguous()
-        else:
-            self.T = n_types
-        self.slot = slot
-        self.origin = origins
-        self.lo, self.hi = box_lo, box_hi
-        self.spacing = spacing
-        self.penalty = penalty
+        blocks = list(grids.unbind(0)) if torch.is_tensor(grids) else list(grids)
+        self.G = grids if torch.is_tensor(grids) else None
+        self.R = len(blocks)
+        self.flat = grids.reshape(-1) if self.G is not None else torch.cat([b.reshape(-1) for b in blocks])
+        self.dims = torch.tensor([list(b.shape[1:]) for b in blocks], dtype=torch.long, device=dev)
+        sizes = torch.tensor([b.numel() for b in blocks], dtype=torch.long, device=dev)
+        self.offs = torch.cumsum(sizes, 0) - sizes
+        self.n = int(self.dims.max())
+        built = blocks[0].shape[0]
+        self.T = built if slot is None else n_types
+        self.slot = (torch.arange(built, device=dev).repeat(self.R, 1) if slot is None else slot)
+        self.origin, self.lo, self.hi = origins, box_lo, box_hi
+        self.spacing, self.penalty = spacing, penalty
         self._lowp = {}
-
-    def lookup(self, x, t, rec_idx, mask=None):
-        return trilinear(self.flat, self.origin, self.lo, self.hi, x, t, rec_idx, mask, self.dims, self.offs,
-                         self.slot, self.spacing, self.penalty)
-
-    def lookup_nearest(self, x, t, rec_idx):
-        """Nearest-grid-point energy (no gradient), grid.py:238-247."""
-        dm = self.dims[rec_idx]
-        f = torch.minimum(((x - self.origin[rec_idx]) / self.spacing).round().clamp(min=0).long(), dm - 1)
-        ny, nz = dm[..., 1], dm[..., 2]
-        base = self.offs[rec_idx] + self.slot[rec_idx, t.clamp(min=0)].clamp(min=0) * (dm[..., 0] * ny * nz)
-        e = self.flat[base + (f[..., 0] * ny + f[..., 1]) * nz + f[..., 2]]
-        lo, hi = self.lo[rec_idx], self.hi[rec_idx]
-        out = (lo - x).clamp(min=0) ** 2 + (x - hi).clamp(min=0) ** 2
-        return e + self.penalty * out.sum(-1)
 
     def storage(self, dtype: str = "f32"):
         """(flat tensor, ADOCK_GRID_* code) of the maps in ``dtype`` ('f32', 'f16', 'bf16'); low-precision copies
@@ -192,9 +141,8 @@ class GridSet:
             return self.flat.float().contiguous(), _lib.ADOCK_GRID_F32
         if dtype not in self._lowp:
             code = {"f16": _lib.ADOCK_GRID_F16, "bf16": _lib.ADOCK_GRID_BF16}[dtype]
-            tdt = {"f16": torch.float16, "bf16": torch.bfloat16}[dtype]
             src = self.flat.float().contiguous()
-            dst = torch.empty(src.shape, dtype=tdt, device=src.device)
+            dst = torch.empty(src.shape, dtype={"f16": torch.float16, "bf16": torch.bfloat16}[dtype], device=src.device)
             with torch.cuda.device(src.device):
                 _lib.call("adock_grid_convert", _lib.ptr(src), _lib.ptr(dst), src.numel(), code, _lib.stream_ptr())
             self._lowp[dtype] = (dst, code)
@@ -205,52 +153,52 @@ def grid_dims(size, spacing):
     return tuple(int(math.ceil(x / spacing)) + 1 for x in size)
 
 
+def _boxes(receptors):
+    """(centre, size, origin = low corner) of every receptor's box, float64."""
+    c = np.array([np.asarray(r["center"], float) for r in receptors])
+    s = np.array([np.asarray(r["size"], float) for r in receptors])
+    return c, s, c - s / 2.0
+
+
+def _f32(a, device):
+    return torch.as_tensor(np.asarray(a, np.float32), device=device)
+
+
 def make_gridset(receptors, sfp, spacing, penalty, device="cuda", per_term=False, cubic=None, lig_types=None,
                  builder=None):
-    """receptors: list of dicts with rec_xyz, rec_types, center, size (grid.py:250-282).
+    """GridSet of receptor dicts (rec_xyz, rec_types, center, size), reference ``grid.py:250-282``.
 
-    cubic=True: common cube n for all receptors (stacked .G). cubic=False (default unless per_term): each receptor
-    gets n_d = ceil(size_d / spacing) + 1 points per axis and, with lig_types, only the ligand's own types plus
-    type 0 (C_H, the Stage-A probe type). ``builder`` replaces ``build_grid`` (same signature)."""
+    cubic (default: per_term): one common cube of n = ceil(max size / spacing) + 1 points per axis for all receptors
+    and all types (stacked ``G``). Otherwise each receptor gets ceil(size_d / spacing) + 1 points per axis and, with
+    ``lig_types`` (one list per receptor), only those types plus type 0 (C_H, the Stage-A probe). ``builder``
+    replaces ``build_grid`` (same signature)."""
     builder = builder or build_grid
     cubic = per_term if cubic is None else cubic
-    T_all = len(sfp["radius"])
-    if lig_types is not None and not cubic:
-        sel = [np.unique(np.concatenate([[0], np.asarray(lt, dtype=np.int64)])) for lt in lig_types]
-    else:
-        sel = [np.arange(T_all)] * len(receptors)
-    slot = -np.ones((len(receptors), T_all), np.int64)
-    for i, st in enumerate(sel):
-        slot[i, st] = np.arange(len(st))
-    n = int(math.ceil(max(max(r["size"]) for r in receptors) / spacing)) + 1
-    grids, origins, lo, hi = [], [], [], []
-    for r, st in zip(receptors, sel):
-        c, s = np.asarray(r["center"], float), np.asarray(r["size"], float)
-        origin = c - s / 2.0
-        nn = n if cubic else grid_dims(s, spacing)
-        grids.append(builder(r["rec_xyz"], r["rec_types"], sfp, origin, spacing, nn, per_term=per_term, device=device,
-                             lig_types=None if cubic else st))
-        origins.append(origin)
-        lo.append(c - s / 2.0)
-        hi.append(c + s / 2.0)
-    tt = lambda a: torch.tensor(np.array(a), dtype=torch.float32, device=device)
+    n_types = len(sfp["radius"])
+    centre, size, origin = _boxes(receptors)
     if cubic:
-        return GridSet(torch.stack(grids), tt(origins), tt(lo), tt(hi), spacing, penalty)
-    return GridSet(grids, tt(origins), tt(lo), tt(hi), spacing, penalty, slot=torch.as_tensor(slot, device=device),
-                   n_types=T_all)
+        n = int(math.ceil(size.max() / spacing)) + 1
+        G = torch.stack([builder(r["rec_xyz"], r["rec_types"], sfp, o, spacing, n, per_term=per_term, device=device,
+                                 lig_types=None) for r, o in zip(receptors, origin)])
+        return GridSet(G, _f32(origin, device), _f32(origin, device), _f32(centre + size / 2, device), spacing,
+                       penalty)
+    types = [np.union1d([0], np.asarray(t, np.int64)) if lig_types is not None else np.arange(n_types)
+             for t in (lig_types if lig_types is not None else [None] * len(receptors))]
+    slot = np.full((len(receptors), n_types), -1, np.int64)
+    for r, t in enumerate(types):
+        slot[r, t] = np.arange(len(t))
+    maps = [builder(r["rec_xyz"], r["rec_types"], sfp, o, spacing, grid_dims(sz, spacing), per_term=per_term,
+                    device=device, lig_types=t) for r, o, sz, t in zip(receptors, origin, size, types)]
+    return GridSet(maps, _f32(origin, device), _f32(origin, device), _f32(centre + size / 2, device), spacing,
+                   penalty, slot=torch.as_tensor(slot, device=device), n_types=n_types)
 
 
 def make_gridset_fit(preps, pot, spacing, penalty, device="cuda", builder=None):
-    """preps: dicts with rec_xyz, rec_ext, center, size; common cube n (gridfit.py:96-108)."""
+    """GridSet of the fitted function's maps (reference ``gridfit.py:96-108``): preps with rec_xyz, rec_ext, center,
+    size; one common cube for all receptors, the compact ligand types of ``pot``."""
     builder = builder or build_grid_fit
-    n = int(math.ceil(max(max(r["size"]) for r in preps) / spacing)) + 1
-    grids, origins, lo, hi = [], [], [], []
-    for r in preps:
-        c, s = np.asarray(r["center"], float), np.asarray(r["size"], float)
-        origin = c - s / 2.0
-        grids.append(builder(r["rec_xyz"], r["rec_ext"], pot, origin, spacing, n, device=device))
-        origins.append(origin)
-        lo.append(c - s / 2.0)
-        hi.append(c + s / 2.0)
-    tt = lambda a: torch.tensor(np.array(a), dtype=torch.float32, device=device)
-    return GridSet(torch.stack(grids), tt(origins), tt(lo), tt(hi), spacing, penalty)
+    centre, size, origin = _boxes(preps)
+    n = int(math.ceil(size.max() / spacing)) + 1
+    G = torch.stack([builder(r["rec_xyz"], r["rec_ext"], pot, o, spacing, n, device=device)
+                     for r, o in zip(preps, origin)])
+    return GridSet(G, _f32(origin, device), _f32(origin, device), _f32(centre + size / 2, device), spacing, penalty)
