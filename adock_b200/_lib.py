@@ -49,7 +49,8 @@ class McArgs(ctypes.Structure):
                 ("bfgs_iters", I), ("temp", F), ("amp_pos", F), ("amp_rot", F), ("seed", ctypes.c_ulonglong),
                 ("step_offset", I), ("exact", I), ("order", P), ("queue", P), ("evals", P), ("variant", I),
                 ("prop", P), ("prop_k", I), ("prop_stats", P), ("log_x", P), ("log_y", P), ("log_n", P),
-                ("log_cap", I), ("prop_frac", F), ("lig_active", P)]
+                ("log_cap", I), ("prop_frac", F), ("lig_active", P),
+                ("prop_tries", I)]
 
 
 SP = ctypes.POINTER

@@ -216,7 +216,7 @@ __global__ void prop_sample_kernel(const int4* info, const int* chain_lig, const
     const int kk = (int)(idx % k);
     const int c = (int)(idx / k);
     const int nt = info[chain_lig[c]].y;
-    const int cid = chain_id[c], step = 64 * segment + kk;
+    const int cid = chain_id[c], step = (k > 64 ? k : 64) * segment + kk;
     const float* o = out + (long long)c * 64;
     const float* s = state + (long long)c * SD;
     float d[26];
@@ -362,6 +362,8 @@ extern "C" int adock_mc(const adock_ligands_t* lig, const adock_work_t* work, co
     M.prop_frac = (mc->prop_frac <= 0.f || mc->prop_frac >= 1.f) ? 1.f : mc->prop_frac;
     M.log_x = (__nv_bfloat16*)mc->log_x; M.log_y = mc->log_y; M.log_n = mc->log_n; M.log_cap = mc->log_cap;
     M.lig_active = mc->lig_active;
+    M.prop_tries = mc->prop_tries > 1 ? mc->prop_tries : 1;
+    ADOCK_CHECK_ARG(!mc->prop || mc->prop_k % M.prop_tries == 0, "prop_k must be a multiple of prop_tries");
     const TypeTables tt = make_tables(sf);
     cudaStream_t st = (cudaStream_t)stream;
     switch (grids->dtype) {
@@ -552,7 +554,7 @@ extern "C" int adock_prop_sample(const adock_ligands_t* lig, const adock_work_t*
                                  const int* chain_id, int n, const float* net_out, const float* state, int SD, int k,
                                  unsigned long long seed, int segment, float* targets, void* stream) {
     ADOCK_CHECK_ARG(lig && work && work->info, "null argument");
-    ADOCK_CHECK_ARG(n >= 0 && k >= 1 && k <= 64, "n must be >= 0 and k in [1, 64]");
+    ADOCK_CHECK_ARG(n >= 0 && k >= 1 && k <= 512, "n must be >= 0 and k in [1, 512]");
     ADOCK_CHECK_ARG(SD >= 7, "SD must be >= 7");
     if (n == 0) return ADOCK_OK;
     ADOCK_CHECK_ARG(chain_lig && chain_id && net_out && state && targets, "null array argument");

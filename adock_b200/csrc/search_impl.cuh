@@ -90,6 +90,7 @@ struct McParams {
     int* log_n;
     int log_cap;
     const int* lig_active;           // [L] or NULL: chains of a ligand with flag 0 are left unchanged
+    int prop_tries;                  // learned steps: candidate targets per step (the lowest-energy one is optimised)
 };
 
 #define PROP_IN 288
@@ -749,8 +750,26 @@ __global__ void __launch_bounds__(128, MINB) mc_kernel(const __grid_constant__ S
             const bool use_prop = M.prop && prop_fail < PROP_FAIL_MAX &&
                                   (M.prop_frac >= 1.f || uniform01(M.seed, cid, sg, 3) < M.prop_frac);
             if (use_prop) {
-                // the proposed target state (drawn around the state the network read at the segment start)
-                const float* mv = M.prop + ((long long)ch * M.prop_k + (st % M.prop_k)) * PROP_MOVE;
+                // the proposed target state (drawn around the state the network read at the segment start); with
+                // several tries per step, each candidate is evaluated once and the lowest-energy one is kept
+                const int T = M.prop_tries > 1 ? M.prop_tries : 1;
+                const float* mv0 = M.prop + ((long long)ch * M.prop_k + (long long)(st % (M.prop_k / T)) * T) * PROP_MOVE;
+                int pick = 0;
+                if (T > 1) {
+                    float e_min = 3.4e38f;
+                    for (int tr = 0; tr < T; ++tr) {
+                        const float* mv = mv0 + (long long)tr * PROP_MOVE;
+                        for (int i = lane; i < S; i += 32) x[i] = cur[i];
+                        __syncwarp();
+                        if (lane < 7) x[lane] = mv[lane];
+                        for (int k = lane; k < c.nt && k < 20; k += 32) x[7 + k] = mv[7 + k];
+                        __syncwarp();
+                        const float et = bfgs<APL, GT>(ws, L, x, 0, c, P, tt, lane, n_eval);   // one evaluation
+                        if (et < e_min) { e_min = et; pick = tr; }
+                    }
+                    wcopy(x, cur, S, lane);
+                }
+                const float* mv = mv0 + (long long)pick * PROP_MOVE;
                 if (lane < 7) x[lane] = mv[lane];
                 for (int k = lane; k < c.nt && k < 20; k += 32) x[7 + k] = mv[7 + k];
             } else {

@@ -169,14 +169,15 @@ class B200KernelProblem:
 
     def run_mc(self, chain_lig, chain_id, cur, cur_e, best, best_e, init_opt, mc_steps, bfgs_iters, temp,
                amp_pos, amp_rot, seed, step_offset, exact=False, nbr=None, nbr_n=None, order=None, variant=None,
-               prop=None, prop_stats=None, log=None, prop_frac=1.0, lig_active=None):
+               prop=None, prop_stats=None, log=None, prop_frac=1.0, lig_active=None, prop_tries=1):
         """In place on cur/cur_e/best/best_e (float32 contiguous CUDA tensors). exact=True with nbr [N, NB] int32 /
         nbr_n [N]: each chain's exact inter energy loops only over its receptor-atom neighbour list.
         variant: MC launch variant (default: the tuned one, else the library default).
         prop: learned moves [N, k, 32] for steps 0..k-1 of this launch (plain MC fallback after 8 rejections);
         prop_stats: int64 [4] counters; log: (x BF16 [cap, 288], y [cap, 32], n int32 [1]) training-data log;
         prop_frac: fraction of steps that take the learned move (the others take the plain random move);
-        lig_active: int32 [L] device flags, chains of ligands with 0 are left unchanged (None: all run)."""
+        lig_active: int32 [L] device flags, chains of ligands with 0 are left unchanged (None: all run);
+        prop_tries: candidate targets per learned step (prop then holds steps x prop_tries targets per chain)."""
         N = cur.shape[0]
         if N == 0:
             return
@@ -208,6 +209,7 @@ class B200KernelProblem:
             assert prop.is_contiguous() and prop.shape[0] == N and prop.shape[2] == 32 and prop.dtype == torch.float32
             a.prop, a.prop_k = _lib.ptr(prop), int(prop.shape[1])
             a.prop_frac = float(prop_frac)
+            a.prop_tries = int(prop_tries)
             keep.append(prop)
         if prop_stats is not None:
             a.prop_stats = _lib.ptr(prop_stats)

@@ -293,7 +293,7 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
     torch.cuda.synchronize(dev)
     # learned variants: (name, segment steps, learned fraction[, training "chain" | "ligand" | "dagger"]): the
     # chain's or the ligand's best pose as target, or the chain network fine-tuned on its own search's moves
-    variants = {v[0]: (v[1], v[2], v[3] if len(v) > 3 else "chain") for v in learned}
+    variants = {v[0]: (v[1], v[2], v[3] if len(v) > 3 else "chain", int(v[4]) if len(v) > 4 else 1) for v in learned}
     X, Yc, Yl = collect(kp_t, cl, ci, cur, ce, best, be, cfg_tr, seed=seed + 1, cap=log_cap, target="both")
     nets = {}
     out["train"] = {"moves": int(X.shape[0]), "epochs": epochs}
@@ -303,7 +303,7 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
     def dagger_name(n):
         return "chain" if n == 0 else ("dagger" if n == 1 else f"dagger{n}")
 
-    targets = {t for (_, _, t) in variants.values()}
+    targets = {t for (_, _, t, _) in variants.values()}
     for n in range(max(rounds(t) for t in targets)):
         targets.add(dagger_name(n))
     for tgt in sorted(targets, key=lambda t: (t == "ligand", rounds(t))):
@@ -347,9 +347,9 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
         ce, be = torch.zeros(cur.shape[0], device=dev), torch.full((cur.shape[0],), float("inf"), device=dev)
         st = {}
         if method in variants:
-            k, frac, tgt = variants[method]
+            k, frac, tgt, tries = variants[method]
             run_mc_segments(kp, nets[tgt], cl, ci, cur, ce, best, be, cfg, seed + 3, prop_k=k, prop_frac=frac,
-                            stats=st)
+                            stats=st, prop_tries=tries)
         else:
             kp.run_mc(cl, ci, cur, ce, best, be, True, steps, cfg["bfgs_iters"], cfg["mc_temperature"],
                       cfg["mc_amp_pos"], cfg["mc_amp_rot"], seed + 3, 0)
@@ -362,7 +362,8 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
 
     ref, ref_ms, ref_st = run("plain_f32", ref_steps)
     results = {}
-    out["learned_variants"] = {n: {"prop_k": k, "prop_frac": f, "target": t} for n, (k, f, t) in variants.items()}
+    out["learned_variants"] = {n: {"prop_k": k, "prop_frac": f, "target": t, "tries": r}
+                               for n, (k, f, t, r) in variants.items()}
     for m in ("plain_f32", *(("plain_f16",) if plain_f16 else ()), *variants):
         for S in (learned_budgets or budgets if m in variants else budgets):
             results[(m, S)] = run(m, S)
@@ -424,22 +425,23 @@ def interp_to_gap(rows, gap):
 
 
 def run_mc_segments(kp, net, chain_lig, chain_id, cur, cur_e, best, best_e, cfg, seed, prop_k=32, init_opt=True,
-                    stats=None, prop_frac=0.3, log=None):
+                    stats=None, prop_frac=0.3, log=None, prop_tries=1):
     """MC with learned proposals: the run is cut into segments of prop_k steps; before each segment the network
     reads every chain's current state and draws prop_k target states per chain around it (adock_prop_sample); a
     step proposes the next of them with probability prop_frac, else it takes the plain random move (and plain MC
     after 8 consecutive rejections of learned proposals). log: the training-data log of run_mc, kept across the
-    segments."""
+    segments. prop_tries > 1: each learned step draws that many targets, evaluates each once and optimises the
+    lowest-energy one."""
     steps = cfg["mc_steps"]
     pst = torch.zeros(4, dtype=torch.int64, device=kp.device)
     for sg in range(math.ceil(steps / prop_k)):
         k = min(prop_k, steps - sg * prop_k)
         feat = kp.prop_features(chain_lig, cur)
         out = net.forward(feat)
-        moves = kp.prop_sample(chain_lig, chain_id, out, cur, k, seed ^ 0x5EEDBA5E, sg)
+        moves = kp.prop_sample(chain_lig, chain_id, out, cur, k * prop_tries, seed ^ 0x5EEDBA5E, sg)
         kp.run_mc(chain_lig, chain_id, cur, cur_e, best, best_e, init_opt and sg == 0, k, cfg["bfgs_iters"],
                   cfg["mc_temperature"], cfg["mc_amp_pos"], cfg["mc_amp_rot"], seed, sg * prop_k, prop=moves,
-                  prop_stats=pst, prop_frac=prop_frac, log=log)
+                  prop_stats=pst, prop_frac=prop_frac, log=log, prop_tries=prop_tries)
     check_gemm("learned-proposal search")
     if stats is not None:
         p, pa, q, qa = pst.tolist()

@@ -56,7 +56,7 @@ def _args():
     ap.add_argument("--ab-train", type=int, default=256, help="fresh ligands for the proposal's training data")
     ap.add_argument("--ab-eval", type=int, default=256, help="held-out ligands for the A/B comparison")
     ap.add_argument("--ab-variants", default="learned_f16:32:0.3",
-                    help="learned variants name:segment_steps:learned_fraction[:chain|ligand|dagger training], "
+                    help="learned variants name:segment_steps:learned_fraction[:chain|ligand|dagger training[:tries]], "
                          "comma separated")
     ap.add_argument("--screen", action="store_true",
                     help="screening comparison on the 8,000-atom receptor with 8-80-atom ligands (FP16 + learned "
@@ -303,7 +303,7 @@ def run_ours(args, rank, world, local_rank):
         dock_screen(rec, box, ligs, cfg, device=dev, stats=st)   # warm-up (allocator, module load)
         barrier()
         e2e_ms, h2d, d2h = [], 0, 0
-        for _ in range(max(1, min(args.steps, 3))):
+        for _ in range(max(1, args.steps)):
             flush.zero_()
             st = {}
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -318,7 +318,9 @@ def run_ours(args, rank, world, local_rank):
         if world > 1:
             t = max_over_ranks(t, device=dev)
         e2e = {"value": args.ligands * world * len(e2e_ms) / (t / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(d2h)}
+               "d2h_bytes_per_step": int(d2h),
+               "spread": [args.ligands * world / (max(e2e_ms) / 1e3), args.ligands * world / (min(e2e_ms) / 1e3)],
+               "repeats": len(e2e_ms)}
 
     # ---- roofline of the dominant kernel (MC + BFGS persistent kernel) ----
     peak, peak_kind = _peaks()
@@ -344,6 +346,7 @@ def run_ours(args, rank, world, local_rank):
            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, shapes of the batched uneven workload)",
            "config": {"workload": WORKLOAD, "ligands_per_gpu": args.ligands, "chains": CHAINS, "mc_steps": args.mc_steps,
                       "l2": "flushed (256 MB write) between timed steps", "parallelism": f"ligand shards x{world}"},
+           "value_spread": [args.ligands * world / (max(step_ms) / 1e3), args.ligands * world / (min(step_ms) / 1e3)],
            "evals_per_s": evals * world / mc_s, "mc_share_of_step": sum(mc_ms) / sum(step_ms),
            "roofline": roof, "clocks": clk, "gpu_launches": launches, "e2e": e2e,
            "mc_autotune": __import__("adock_b200.autotune", fromlist=["cached"]).cached()}
@@ -353,7 +356,8 @@ def run_ours(args, rank, world, local_rank):
         out_v = []
         for v in spec.split(","):
             f = v.split(":")
-            out_v.append((f[0], int(f[1]), float(f[2])) + ((f[3],) if len(f) > 3 else ()))
+            out_v.append((f[0], int(f[1]), float(f[2])) + ((f[3],) if len(f) > 3 else ())
+                         + ((int(f[4]),) if len(f) > 4 else ()))
         return out_v
 
     variants = parse_variants(args.ab_variants)

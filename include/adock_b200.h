@@ -131,6 +131,10 @@ typedef struct {
     float prop_frac;           /* with proposals: fraction of steps that take the learned move (<= 0 or >= 1: all) */
     const int* lig_active;     /* dev [L] or NULL: chains of ligands whose flag is 0 are skipped (left unchanged);
                                   replaces the host-side compaction of active chains (search.py:614-627) */
+    int prop_tries;            /* learned steps (no reference counterpart): candidate targets per step; each is
+                                  evaluated once and BFGS runs from the lowest-energy one. prop then holds
+                                  prop_k = steps x prop_tries targets per chain, the tries of a step consecutive.
+                                  <= 1: one target per step */
 } adock_mc_args_t;
 
 /* ------------------------------------------------------------------------------------------------ misc */
@@ -282,7 +286,7 @@ int adock_prop_features(const adock_ligands_t* lig, const adock_work_t* work, co
  * around the states state [n, SD] the network read: move = mean + max(exp(log_sd), floor) * z, z standard normal
  * from a counter-based stream of (seed, chain_id, segment, slot), applied to the state (translation added,
  * rotation vector composed on the left of q, torsion deltas added; torsions past a ligand's count keep their
- * value). k <= 64. */
+ * value). k <= 512. */
 int adock_prop_sample(const adock_ligands_t* lig, const adock_work_t* work, const int* chain_lig, const int* chain_id,
                       int n, const float* net_out, const float* state, int SD, int k, unsigned long long seed,
                       int segment, float* targets, void* stream);
