@@ -47,3 +47,39 @@ def test_version_and_argument_errors_without_gpu():
         sf.n_types = 18
         w = _lib.Work()
         _lib.call("adock_prepare", lig, sf, w, None)
+
+
+def test_pipeline_entry_points_reject_bad_arguments_without_gpu():
+    """The device-pipeline entry points check sizes and limits on the host and refuse with a message: start
+    selection beyond 16,384 (conformer, rotation) totals, clustering beyond 4,096 poses or 32 representatives,
+    conformer counts out of range, and grid cell lists too coarse for the cutoff."""
+    from adock_b200 import _lib
+    if not _lib.LIB_PATH.exists():
+        pytest.skip("libadock_b200.so not built")
+    p = ctypes.c_void_p(8)      # never dereferenced: every call below fails its argument check first
+    with pytest.raises(RuntimeError, match="16384"):
+        _lib.call("adock_select_starts", 1, 64, 512, 8, 4, p, p, p, p, p, p, None, 10, p, None, None)
+    w = _lib.Work()
+    w.info = 8
+    with pytest.raises(RuntimeError, match="4096"):
+        _lib.call("adock_cluster", w, 1, 5000, p, p, 64, 2.0, 9, p, p, None)
+    with pytest.raises(RuntimeError, match="n_out"):
+        _lib.call("adock_cluster", w, 1, 16, p, p, 64, 2.0, 40, p, p, None)
+    lig = _lib.Ligands()
+    lig.L, lig.AM, lig.KM, lig.P = 1, 64, 8, 1
+    sf = _lib.SF()
+    sf.n_types = 18
+    with pytest.raises(RuntimeError, match="NT"):
+        _lib.call("adock_conformers", lig, _lib.Work(), sf, 0, 1, 0, p, p, p, None)
+    with pytest.raises(RuntimeError, match="C must"):
+        _lib.call("adock_conformers", lig, _lib.Work(), sf, 8, 9, 0, p, p, p, None)
+    dims = (ctypes.c_int * 3)(4, 4, 4)
+    org = (ctypes.c_float * 3)(0, 0, 0)
+    prm = (ctypes.c_float * 15)(8.0, 0, 0.5, 3, 2, 0, 0.5, 1.5, -0.7, 0, -0.035, -0.005, 0.84, -0.035, -0.587)
+    lt = (ctypes.c_int * 1)(0)
+    tab = (ctypes.c_int * 18)()
+    rad = (ctypes.c_float * 18)(*([1.9] * 18))
+    with pytest.raises(RuntimeError, match="cell size"):
+        _lib.call("adock_grid_vina_cells", p, p, 10, p, ctypes.addressof(dims), ctypes.addressof(org), 1.0,
+                  ctypes.addressof(rad), ctypes.addressof(tab), ctypes.addressof(tab), ctypes.addressof(tab), 18,
+                  ctypes.addressof(lt), 1, 0.0, 0.0, 0.0, 0.375, 8, 8, 8, ctypes.addressof(prm), 0, p, None)
