@@ -25,7 +25,6 @@ namespace adock {
 #define ADOCK_COLD_ATTR __forceinline__
 #endif
 #define PAIR_ROUNDS_MAX 256   // pair schedule: at most 256 rounds of 32 (8,192 pairs) are reordered
-#define PAIR_QUEUE 64         // per-warp ring of intra pairs found inside the cutoff, evaluated 32 at a time
 
 struct SearchParams {
     // B200 working layout
@@ -113,14 +112,12 @@ __device__ __forceinline__ void stage_tables(TypeTables& dst, const TypeTables& 
 // ------------------------------------------------------------------------------------------ per-warp workspace
 // Float offsets of the per-warp shared workspace for a given AM / KM (float4 arrays first).
 struct WSLayout {
-    int X, FF, qd, qr, ap, au, tp, tu, mk, ax, cs, sn, H, x, xn, xo, cur, best, g, gn, go, p, y, mhy, total;
+    int X, FF, ap, au, tp, tu, mk, ax, cs, sn, H, x, xn, xo, cur, best, g, gn, go, p, y, mhy, total;
     __host__ __device__ WSLayout(int AM, int KM) {
         const int DM = 6 + KM, SD = 7 + KM;
         int o = 0;
         X = o; o += 3 * AM;    // world coordinates, [3][AM] (x, y, z arrays)
         FF = o; o += 3 * AM;   // forces, [3][AM]
-        qd = o; o += 4 * PAIR_QUEUE;   // in-cutoff pair queue: separation (x, y, z) and r^2 (float4)
-        qr = o; o += 2 * PAIR_QUEUE;   // in-cutoff pair queue: pair record (int2)
         ap = o; o += 4 * KM;
         au = o; o += 4 * KM;
         tp = o; o += 4 * KM;
@@ -250,22 +247,24 @@ __device__ __forceinline__ float trilinear(const GT* G, int ny, int nz, const fl
     return e;
 }
 
-// Intra-ligand pair term of one queued pair (record pr, separation d.xyz = X_i - X_j, d.w = r^2): energy, and the
-// force added into both atoms' entries. Positions and forces are three arrays of AM floats each (x, y, z), so that
-// 32 lanes touching 32 different atoms hit 32 different shared-memory banks (a float4 per atom would put the x
-// components of 32 atoms on 8 banks).
+// Intra-ligand pair term of one scheduled slot: energy, and the force added into both atoms' entries. Positions X
+// and forces F are three arrays of AM floats each (x, y, z), so that 32 lanes touching 32 different atoms hit 32
+// different shared-memory banks (a float4 per atom would put the x components of 32 atoms on 8 banks).
 template <int AM>
-__device__ __forceinline__ float pair_eval(int2 pr, float4 d, float* F, const PairPrm& pp) {
+__device__ __forceinline__ float pair_slot(int2 pr, const float* X, float* F, const PairPrm& pp) {
+    if (pr.x < 0) return 0.f;
     const int i = pr.x & 0xff, j = (pr.x >> 8) & 0xff, fl = pr.x >> 16;
+    const float rx = X[i] - X[j], ry = X[AM + i] - X[AM + j], rz = X[2 * AM + i] - X[2 * AM + j];
     // r and 1/r from one reciprocal square root; clamping r^2 at 1e-12 is the reference's max(r, 1e-6)
-    const float rinv = rsqrtf(fmaxf(d.w, 1e-12f));
-    const float r = d.w * rinv;
+    const float r2 = rx * rx + ry * ry + rz * rz;
+    const float rinv = rsqrtf(fmaxf(r2, 1e-12f));
+    const float r = r2 * rinv;
     if (r >= pp.cutoff) return 0.f;
     float de;
     const float e = pair_energy(r, __int_as_float(pr.y), fl, pp, de);
     const float sc = de * rinv;
-    atomicAdd(F + i, sc * d.x); atomicAdd(F + AM + i, sc * d.y); atomicAdd(F + 2 * AM + i, sc * d.z);
-    atomicAdd(F + j, -sc * d.x); atomicAdd(F + AM + j, -sc * d.y); atomicAdd(F + 2 * AM + j, -sc * d.z);
+    atomicAdd(F + i, sc * rx); atomicAdd(F + AM + i, sc * ry); atomicAdd(F + 2 * AM + i, sc * rz);
+    atomicAdd(F + j, -sc * rx); atomicAdd(F + AM + j, -sc * ry); atomicAdd(F + 2 * AM + j, -sc * rz);
     return e;
 }
 
@@ -370,52 +369,20 @@ __device__ __forceinline__ float eval_eg(float* ws, const WSLayout& L, const flo
         }
     }
     __syncwarp();
-    // intra-ligand pairs, in two stages. Stage 1 walks the scheduled rounds of 32 (adock_prepare: an atom appears at
-    // most once per round where possible) and computes each pair's separation; the pairs inside the cutoff (about
-    // half of them: the rest contribute nothing) are appended to a per-warp ring by ballot. Stage 2 evaluates the
-    // terms and force atomics of 32 queued pairs whenever the ring holds that many, so its lanes are all busy.
-    // Records of the next two rounds are loaded ahead.
+    // intra-ligand pairs, scheduled in rounds of 32 in which an atom appears at most once (adock_prepare), so the
+    // force atomics of one round do not collide; two rounds in flight per iteration
+    // the next two rounds' records are loaded while the current two are evaluated
     {
-        float4* qd = (float4*)(ws + L.qd);
-        int2* qr = (int2*)(ws + L.qr);
-        const float keep2 = P.pp.cutoff * P.pp.cutoff * 1.0001f;   // stage 1 keeps a margin; stage 2 tests r < cutoff
-        const unsigned below = (1u << lane) - 1u;
         const int2 none = make_int2(-1, 0);
         int2 pa = c.nrounds > 0 ? c.pairs[lane] : none;
         int2 pb = c.nrounds > 1 ? c.pairs[32 + lane] : none;
-        int head = 0, fill = 0;
-        for (int r = 0; r < c.nrounds; ++r) {
-            const int2 pr = pa;
-            pa = pb;
-            pb = (r + 2 < c.nrounds) ? c.pairs[(r + 2) * 32 + lane] : none;
-            bool keep = false;
-            float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (pr.x >= 0) {
-                const int i = pr.x & 0xff, j = (pr.x >> 8) & 0xff;
-                d.x = X[i] - X[j]; d.y = X[AM + i] - X[AM + j]; d.z = X[2 * AM + i] - X[2 * AM + j];
-                d.w = d.x * d.x + d.y * d.y + d.z * d.z;
-                keep = d.w < keep2;
-            }
-            const unsigned bal = __ballot_sync(0xffffffffu, keep);
-            if (keep) {
-                const int q = (head + fill + __popc(bal & below)) & (PAIR_QUEUE - 1);
-                qd[q] = d;
-                qr[q] = pr;
-            }
-            fill += __popc(bal);
-            if (fill >= 32) {
-                __syncwarp();
-                const int q = (head + lane) & (PAIR_QUEUE - 1);
-                e += pair_eval<AM>(qr[q], qd[q], FF, P.pp);
-                head = (head + 32) & (PAIR_QUEUE - 1);
-                fill -= 32;
-                __syncwarp();   // the ring slots just read may be refilled by the next round
-            }
-        }
-        __syncwarp();
-        if (lane < fill) {
-            const int q = (head + lane) & (PAIR_QUEUE - 1);
-            e += pair_eval<AM>(qr[q], qd[q], FF, P.pp);
+        for (int r = 0; r < c.nrounds; r += 2) {
+            const int2 qa = (r + 2 < c.nrounds) ? c.pairs[(r + 2) * 32 + lane] : none;
+            const int2 qb = (r + 3 < c.nrounds) ? c.pairs[(r + 3) * 32 + lane] : none;
+            e += pair_slot<AM>(pa, X, FF, P.pp);
+            e += pair_slot<AM>(pb, X, FF, P.pp);
+            pa = qa;
+            pb = qb;
         }
     }
     // world torsion axes (axis atoms' current positions)
@@ -684,6 +651,15 @@ __device__ ADOCK_COLD_ATTR void prop_features(const SearchParams& P, int l, cons
     __syncwarp();
 }
 
+// True on all lanes when a learned target state (t, q and the ligand's first 20 torsions in x) is finite. A non-finite
+// target is never optimised: clamped map lookups and ramps can give non-finite coordinates a finite energy.
+__device__ __forceinline__ bool target_finite(const float* x, int nt, int lane) {
+    bool ok = true;
+    if (lane < 7) ok = isfinite(x[lane]);
+    for (int k = lane; k < nt && k < 20; k += 32) ok = ok && isfinite(x[7 + k]);
+    return __all_sync(0xffffffffu, ok);
+}
+
 // Training-log row of a state (lane 0 writes): t (3), q (4), theta 0..19 (0 past the torsion count), torsion
 // count at 27, chain index at 28; the training target (the move to a later state of the same chain) is computed
 // after the run.
@@ -749,6 +725,7 @@ __global__ void __launch_bounds__(128, MINB) mc_kernel(const __grid_constant__ S
             // learned move while the proposal has not failed PROP_FAIL_MAX times in a row, else plain MC
             const bool use_prop = M.prop && prop_fail < PROP_FAIL_MAX &&
                                   (M.prop_frac >= 1.f || uniform01(M.seed, cid, sg, 3) < M.prop_frac);
+            bool skip = false;   // a non-finite learned target: rejected without optimisation
             if (use_prop) {
                 // the proposed target state (drawn around the state the network read at the segment start); with
                 // several tries per step, each candidate is evaluated once and the lowest-energy one is kept
@@ -764,6 +741,7 @@ __global__ void __launch_bounds__(128, MINB) mc_kernel(const __grid_constant__ S
                         if (lane < 7) x[lane] = mv[lane];
                         for (int k = lane; k < c.nt && k < 20; k += 32) x[7 + k] = mv[7 + k];
                         __syncwarp();
+                        if (!target_finite(x, c.nt, lane)) continue;
                         const float et = bfgs<APL, GT>(ws, L, x, 0, c, P, tt, lane, n_eval);   // one evaluation
                         if (et < e_min) { e_min = et; pick = tr; }
                     }
@@ -772,6 +750,8 @@ __global__ void __launch_bounds__(128, MINB) mc_kernel(const __grid_constant__ S
                 const float* mv = mv0 + (long long)pick * PROP_MOVE;
                 if (lane < 7) x[lane] = mv[lane];
                 for (int k = lane; k < c.nt && k < 20; k += 32) x[7 + k] = mv[7 + k];
+                __syncwarp();
+                skip = !target_finite(x, c.nt, lane);
             } else {
                 const int nm = 2 + c.nt;
                 const int which = min((int)(uniform01(M.seed, cid, sg, 0) * nm), nm - 1);
@@ -790,8 +770,9 @@ __global__ void __launch_bounds__(128, MINB) mc_kernel(const __grid_constant__ S
                 }
             }
             __syncwarp();
-            const float en = bfgs<APL, GT>(ws, L, x, iters, c, P, tt, lane, n_eval);
-            const bool accept = (en < ec) || (uniform01(M.seed, cid, sg, 2) < __expf((ec - en) / M.temp));
+            const float en = skip ? 3.4e38f : bfgs<APL, GT>(ws, L, x, iters, c, P, tt, lane, n_eval);
+            const bool accept =
+                isfinite(en) && ((en < ec) || (uniform01(M.seed, cid, sg, 2) < __expf((ec - en) / M.temp)));
             if (use_prop) { ++n_prop; n_prop_acc += accept; } else { ++n_plain; n_plain_acc += accept; }
             prop_fail = accept ? 0 : (use_prop ? prop_fail + 1 : prop_fail);
             if (accept && en < ec && M.log_x) {   // training data: features of the pre-move state + the move

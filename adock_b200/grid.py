@@ -52,13 +52,15 @@ class CellList:
                 np.ascontiguousarray(self.origin, np.float32), float(self.size))
 
 
-def build_grid(rec_xyz, rec_types, sfp, origin, spacing, n, lig_types=None, per_term=False, device="cuda"):
-    """Return torch tensor [T, nx, ny, nz] (or [5, T, nx, ny, nz] unweighted if per_term) on ``device``.
+def _dims3(n):
+    return tuple(map(int, (n,) * 3 if np.isscalar(n) else n))
 
-    n: int or (nx, ny, nz). lig_types: XS type indices to build (default: all types)."""
-    if np.isscalar(n):
-        n = (int(n),) * 3
-    nx, ny, nz = map(int, n)
+
+def prepare_grid(rec_xyz, rec_types, sfp, origin, spacing, n, lig_types=None, per_term=False, device="cuda"):
+    """The Vina map build split into its host preparation (cell list, device copies of the receptor and tables)
+    and a ``launch(out)`` that only issues the kernel into ``out`` (flat float32 tensor of ``size`` elements).
+    Returns (launch, size, shape)."""
+    nx, ny, nz = _dims3(n)
     T = len(sfp["radius"])
     lig_types = np.arange(T, dtype=np.int32) if lig_types is None else np.asarray(lig_types, dtype=np.int32)
     assert len(lig_types) <= MAX_TYPES
@@ -69,28 +71,37 @@ def build_grid(rec_xyz, rec_types, sfp, origin, spacing, n, lig_types=None, per_
     rt = torch.as_tensor(np.ascontiguousarray(np.asarray(rec_types)[cells.order], np.int32), device=dev)
     cstart, cdims, corg, csize = cells.args(dev)
     nlt = len(lig_types)
-    out = torch.empty(((5 if per_term else 1) * nlt * nx * ny * nz,), dtype=torch.float32, device=dev)
     tabs = [np.ascontiguousarray(sfp[k], np.int32) for k in ("hydrophobic", "donor", "acceptor")]
     rad = np.ascontiguousarray(sfp["radius"], np.float32)
     prm = grid_prm(sfp)
-    with torch.cuda.device(dev):
-        _lib.call("adock_grid_vina_cells", _lib.ptr(rx), _lib.ptr(rt), len(rx), _lib.ptr(cstart), _lib.ptr(cdims),
-                  _lib.ptr(corg), csize, _lib.ptr(rad), _lib.ptr(tabs[0]),
-                  _lib.ptr(tabs[1]), _lib.ptr(tabs[2]), T, _lib.ptr(lig_types), nlt, float(origin[0]),
-                  float(origin[1]), float(origin[2]), float(spacing), nx, ny, nz, _lib.ptr(prm), int(per_term),
-                  _lib.ptr(out), _lib.stream_ptr())
+    o = [float(x) for x in origin]
+
+    def launch(out):
+        with torch.cuda.device(dev):
+            _lib.call("adock_grid_vina_cells", _lib.ptr(rx), _lib.ptr(rt), len(rx), _lib.ptr(cstart),
+                      _lib.ptr(cdims), _lib.ptr(corg), csize, _lib.ptr(rad), _lib.ptr(tabs[0]), _lib.ptr(tabs[1]),
+                      _lib.ptr(tabs[2]), T, _lib.ptr(lig_types), nlt, o[0], o[1], o[2], float(spacing), nx, ny, nz,
+                      _lib.ptr(prm), int(per_term), _lib.ptr(out), _lib.stream_ptr())
+        return out
+
     shape = ((5, nlt) if per_term else (nlt,)) + (nx, ny, nz)
-    return out.view(shape)
+    return launch, int(np.prod(shape)), shape
 
 
-def build_grid_fit(rec_xyz, rec_ext, pot, origin, spacing, n, device="cuda"):
-    """Grid [TL, n, n, n] of the fitted inter energy for the compact ligand types of ``pot`` (FittedPotential)."""
+def build_grid(rec_xyz, rec_types, sfp, origin, spacing, n, lig_types=None, per_term=False, device="cuda"):
+    """Return torch tensor [T, nx, ny, nz] (or [5, T, nx, ny, nz] unweighted if per_term) on ``device``.
+
+    n: int or (nx, ny, nz). lig_types: XS type indices to build (default: all types)."""
+    launch, size, shape = prepare_grid(rec_xyz, rec_types, sfp, origin, spacing, n, lig_types, per_term, device)
+    return launch(torch.empty(size, dtype=torch.float32, device=_cuda_device(device))).view(shape)
+
+
+def prepare_grid_fit(rec_xyz, rec_ext, pot, origin, spacing, n, device="cuda"):
+    """``build_grid_fit`` split like ``prepare_grid``: returns (launch, size, shape)."""
     spec = pot.spec
     nlt = pot.TL
     assert nlt <= MAX_LT
-    if np.isscalar(n):
-        n = (int(n),) * 3
-    nx, ny, nz = map(int, n)
+    nx, ny, nz = _dims3(n)
     dev = _cuda_device(device)
     xyz = np.ascontiguousarray(rec_xyz, np.float32).reshape(-1, 3)
     cells = CellList(xyz, float(spec.cutoff), float(spacing))
@@ -101,13 +112,22 @@ def build_grid_fit(rec_xyz, rec_ext, pot, origin, spacing, n, device="cuda"):
     rad_rec = torch.as_tensor(np.ascontiguousarray(spec.rec_radius, np.float32), device=dev)
     rad_lig = np.ascontiguousarray(pot.radius, np.float32)
     prm = spec.grid_prm()
-    out = torch.empty((nlt * nx * ny * nz,), dtype=torch.float32, device=dev)
-    with torch.cuda.device(dev):
-        _lib.call("adock_grid_fit_cells", _lib.ptr(rx), _lib.ptr(re), len(rx), _lib.ptr(cstart), _lib.ptr(cdims),
-                  _lib.ptr(corg), csize, _lib.ptr(rad_rec), int(W.shape[0]),
-                  _lib.ptr(rad_lig), nlt, _lib.ptr(W), float(origin[0]), float(origin[1]), float(origin[2]),
-                  float(spacing), nx, ny, nz, _lib.ptr(prm), _lib.ptr(out), _lib.stream_ptr())
-    return out.view(nlt, nx, ny, nz)
+    o = [float(x) for x in origin]
+
+    def launch(out):
+        with torch.cuda.device(dev):
+            _lib.call("adock_grid_fit_cells", _lib.ptr(rx), _lib.ptr(re), len(rx), _lib.ptr(cstart), _lib.ptr(cdims),
+                      _lib.ptr(corg), csize, _lib.ptr(rad_rec), int(W.shape[0]), _lib.ptr(rad_lig), nlt, _lib.ptr(W),
+                      o[0], o[1], o[2], float(spacing), nx, ny, nz, _lib.ptr(prm), _lib.ptr(out), _lib.stream_ptr())
+        return out
+
+    return launch, nlt * nx * ny * nz, (nlt, nx, ny, nz)
+
+
+def build_grid_fit(rec_xyz, rec_ext, pot, origin, spacing, n, device="cuda"):
+    """Grid [TL, n, n, n] of the fitted inter energy for the compact ligand types of ``pot`` (FittedPotential)."""
+    launch, size, shape = prepare_grid_fit(rec_xyz, rec_ext, pot, origin, spacing, n, device)
+    return launch(torch.empty(size, dtype=torch.float32, device=_cuda_device(device))).view(shape)
 
 
 class GridSet:

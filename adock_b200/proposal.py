@@ -205,14 +205,26 @@ def collect(kp, chain_lig, chain_id, cur, cur_e, best, best_e, cfg, seed, cap, i
     n = min(int(ln), cap)
     states = ly[:n]
     ch = states[:, 28].long()
+    ok = torch.isfinite(states[:, :27]).all(1) & torch.isfinite(best[ch]).all(1)
     y_chain = y_lig = None
     if target in ("chain", "both"):
         y_chain = moves_to(states, best[ch])
     if target in ("ligand", "both"):
         y_lig = moves_to(states, best[ligand_best_chain(chain_lig, best_e)[chain_lig.long()[ch]]])
+    keep = _finite_rows(lx[:n], ok, y_chain, y_lig)
     if target == "both":
-        return lx[:n], y_chain, y_lig
-    return lx[:n], (y_chain if target == "chain" else y_lig)
+        return lx[:n][keep], y_chain[keep], y_lig[keep]
+    return lx[:n][keep], (y_chain if target == "chain" else y_lig)[keep]
+
+
+def _finite_rows(X, ok, *Ys):
+    """Rows of a training batch whose features, state and targets are all finite (a row with a non-finite value
+    would turn the whole network into NaN at the first gradient step)."""
+    keep = ok & torch.isfinite(X.float()).all(1)
+    for Y in Ys:
+        if Y is not None:
+            keep &= torch.isfinite(Y).all(1)
+    return keep
 
 
 def collect_learned(kp, net, chain_lig, chain_id, cur, cfg, seed, cap, prop_k=32, prop_frac=0.3):
@@ -229,7 +241,10 @@ def collect_learned(kp, net, chain_lig, chain_id, cur, cfg, seed, cap, prop_k=32
                     log=(lx, ly, ln))
     n = min(int(ln), cap)
     states = ly[:n]
-    return lx[:n], moves_to(states, best[states[:, 28].long()])
+    tgt = best[states[:, 28].long()]
+    Y = moves_to(states, tgt)
+    keep = _finite_rows(lx[:n], torch.isfinite(states[:, :27]).all(1) & torch.isfinite(tgt).all(1), Y)
+    return lx[:n][keep], Y[keep]
 
 
 def _starts(prob, kp, cfg, seed):

@@ -435,7 +435,7 @@ def _grid_and_precision(dev, ligs):
     import torch
     from scipy.spatial import cKDTree
     from adock_b200 import params, synth
-    from adock_b200.grid import build_grid, build_grid_fit, grid_dims
+    from adock_b200.grid import build_grid, build_grid_fit, grid_dims, prepare_grid, prepare_grid_fit
     from adock_b200.precision import precision_report
     rec2 = synth.config_receptor(2)
     sfp = params.sf_params("vina")
@@ -459,14 +459,22 @@ def _grid_and_precision(dev, ligs):
 
     ms_vina = timed(lambda: build_grid(rec2["rec_xyz"], rec2["rec_types"], sfp, o, params.GRID_SPACING, n, lt, device=dev))
     ms_fit = timed(lambda: build_grid_fit(rec2["rec_xyz"], rext, pot, o, params.GRID_SPACING, n, device=dev))
+    # the kernels alone: launches back to back on prepared inputs (the calls above include the host preparation)
+    lv, size_v, _ = prepare_grid(rec2["rec_xyz"], rec2["rec_types"], sfp, o, params.GRID_SPACING, n, lt, device=dev)
+    lf, size_f, _ = prepare_grid_fit(rec2["rec_xyz"], rext, pot, o, params.GRID_SPACING, n, device=dev)
+    out_v = torch.empty(size_v, device=dev)
+    out_f = torch.empty(size_f, device=dev)
+    kms_vina = timed(lambda: lv(out_v), reps=20)
+    kms_fit = timed(lambda: lf(out_f), reps=20)
     # (point, receptor atom) pairs within the 8 A cutoff: the builder's algorithmic work per type
     axes = [o[d] + params.GRID_SPACING * np.arange(n[d]) for d in range(3)]
     pts = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, 3)
     pairs = int(cKDTree(rec2["rec_xyz"]).count_neighbors(cKDTree(pts), 8.0 - 1e-6))
     pte = pairs * len(lt)
     return {"receptor": "8000 atoms, 60 A cube; 30 A box, %dx%dx%d points" % tuple(n), "types": len(lt),
-            "vina_ms": ms_vina, "fitted_ms": ms_fit, "point_atom_pairs": pairs,
-            "vina_pair_type_evals_per_s": pte / (ms_vina / 1e3), "fitted_pair_type_evals_per_s": pte / (ms_fit / 1e3),
+            "vina_ms": ms_vina, "fitted_ms": ms_fit, "vina_kernel_ms": kms_vina, "fitted_kernel_ms": kms_fit,
+            "point_atom_pairs": pairs,
+            "vina_pair_type_evals_per_s": pte / (kms_vina / 1e3), "fitted_pair_type_evals_per_s": pte / (kms_fit / 1e3),
             "precision_100k_poses": precision_report(rec2, ligs, 100_000, device=dev)}
 
 

@@ -2,13 +2,14 @@
 
 The differences are taken in float64 on the device (adock_rescore64: the same energy as adock_eg, float64
 kinematics, the same maps or receptor atoms; the test first checks that the two energies agree), with steps of
-1e-4 A / 1e-4 rad on every state component: translation, rotation (a rotation vector composed on the left of the
+2e-5 A / 2e-5 rad on every state component: translation, rotation (a rotation vector composed on the left of the
 quaternion, the convention of the torque components) and each torsion. The state is float32, so each difference
 is divided by the perturbation actually stored (for the rotation: the rotation vector between the two stored
 quaternions, and the gradient is projected on it).
 
 Components whose perturbation moves an atom across a grid cell (grid mode), or a ligand-receptor (exact mode) or
-intra-ligand pair across the 8 A cutoff, are masked: there the energy has a kink or a step. This follows the
+intra-ligand pair across the 8 A cutoff or an end of its hydrophobic or H-bond ramp, are masked: there the energy
+has a step or a kink. This follows the
 reference's checks of the lookup gradient (tests/test_scoring_grid.py:122-140) and of the pose gradient
 (tests/test_ligand.py:74-110). Bar: per pose ||fd - g|| / max(||g||, 1) < 1e-3 over the unmasked components.
 """
@@ -19,7 +20,7 @@ import torch
 from helpers import ligands, lig_types, make_problem, oracle_grid, random_states, receptor, rel_close
 
 pytestmark = pytest.mark.gpu
-H = 1e-4
+H = 2e-5
 
 
 def _qmul(a, b):
@@ -67,23 +68,40 @@ def _perturbations(st, nt):
     return plus, minus, step
 
 
-def _kinks(model, l, plus, minus, exact, gs, rec_xyz):
-    """[N, D] True where the perturbation crosses a cell boundary / a cutoff (float64 oracle kinematics)."""
+def _crossing(model, dp, dm, rp, rm, ti, tj):
+    """True where a pair's perturbation crosses a point where its energy has a step or a kink: the cutoff, the ends
+    of the hydrophobic ramp (hydrophobic pairs) or of the H-bond ramp (donor-acceptor pairs)."""
+    bad = (rp < model.cutoff) != (rm < model.cutoff)
+    hyd = model.hyd[ti] & model.hyd[tj]
+    hb = (model.don[ti] & model.acc[tj]) | (model.acc[ti] & model.don[tj])
+    for edge, on in ((model.hyd_good, hyd), (model.hyd_bad, hyd), (model.hb_good, hb), (model.hb_bad, hb)):
+        bad |= on & ((dp < edge) != (dm < edge))
+    return bad
+
+
+def _kinks(model, l, plus, minus, exact, gs, rec_xyz, rec_types):
+    """[N, D] True where the perturbation crosses a grid cell (grid mode), or a pair (intra, and ligand-receptor in
+    exact mode) crosses its cutoff or a ramp end (float64 oracle kinematics)."""
     N, D, SD = plus.shape
     Xp = model.pose_heavy(l, plus.reshape(-1, SD)).reshape(N, D, -1, 3)
     Xm = model.pose_heavy(l, minus.reshape(-1, SD)).reshape(N, D, -1, 3)
+    na = Xp.shape[2]
+    tl = model.typ[l, :na]
     bad = np.zeros((N, D), bool)
     npairs = int(model.np[l])
     if npairs:
         i, j = model.pr[l, :npairs, 0], model.pr[l, :npairs, 1]
         rp = np.linalg.norm(Xp[..., i, :] - Xp[..., j, :], axis=-1)
         rm = np.linalg.norm(Xm[..., i, :] - Xm[..., j, :], axis=-1)
-        bad |= ((rp < model.cutoff) != (rm < model.cutoff)).any(-1)
+        rs = model.radius[tl[i]] + model.radius[tl[j]]
+        bad |= _crossing(model, rp - rs, rm - rs, rp, rm, tl[i], tl[j]).any(-1)
     if exact:
+        rt = np.asarray(rec_types, np.int64)
+        rs = model.radius[tl][:, None] + model.radius[rt][None, :]
         for n in range(N):
-            dp = np.linalg.norm(Xp[n][:, :, None] - rec_xyz[None, None], axis=-1)
-            dm = np.linalg.norm(Xm[n][:, :, None] - rec_xyz[None, None], axis=-1)
-            bad[n] |= ((dp < model.cutoff) != (dm < model.cutoff)).any((-1, -2))
+            rp = np.linalg.norm(Xp[n][:, :, None] - rec_xyz[None, None], axis=-1)
+            rm = np.linalg.norm(Xm[n][:, :, None] - rec_xyz[None, None], axis=-1)
+            bad[n] |= _crossing(model, rp - rs, rm - rs, rp, rm, tl[:, None], rt[None, :]).any((-1, -2))
     else:
         dims = gs.dims[0].numpy()
         cell = lambda X: np.floor(np.minimum(np.maximum((X - gs.origin[0].numpy()) / gs.spacing, 0), dims - 1 - 1e-4))
@@ -131,7 +149,7 @@ def test_gradient_matches_central_differences(exact, kind):
                                gl[:, 6:] * step[:, 6:, 0]], 1)
         size = np.linalg.norm(step, axis=-1)
         fd, an = dE / size, pred / size
-        bad = _kinks(model, l, plus, minus, exact, pc.gs, rec["rec_xyz"].astype(np.float64))
+        bad = _kinks(model, l, plus, minus, exact, pc.gs, rec["rec_xyz"].astype(np.float64), rec["rec_types"])
         fd, an = np.where(bad, 0.0, fd), np.where(bad, 0.0, an)
         err = np.linalg.norm(fd - an, axis=1) / np.maximum(np.linalg.norm(an, axis=1), 1.0)
         assert err.max() < 1e-3, (l, err.max(), bad.mean())
