@@ -45,6 +45,8 @@ def _args():
     ap.add_argument("--ligands", type=int, default=N_LIGANDS)
     ap.add_argument("--mc-steps", type=int, default=MC_STEPS)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--mc-variant", type=int, default=0,
+                    help="MC launch variant (1-3: 4, 6 or 8 resident blocks per SM); 0 = the autotuner's choice")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the map-builder / map-precision section")
     ap.add_argument("--no-learned", action="store_true",
@@ -264,6 +266,10 @@ def run_ours(args, rank, world, local_rank):
     bc = torch.tensor(rec["center"], dtype=torch.float32, device=dev)[None].expand(len(ligs), 3)
     bs = [rec["size"]] * len(ligs)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # > 126 MB L2
+
+    if args.mc_variant:
+        cfg = dict(cfg, autotune=False)
+        kp.mc_variant = args.mc_variant
 
     def step(stats):
         kp.evals.zero_()
