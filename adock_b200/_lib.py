@@ -50,7 +50,7 @@ class McArgs(ctypes.Structure):
                 ("step_offset", I), ("exact", I), ("order", P), ("queue", P), ("evals", P), ("variant", I),
                 ("prop", P), ("prop_k", I), ("prop_stats", P), ("log_x", P), ("log_y", P), ("log_n", P),
                 ("log_cap", I), ("prop_frac", F), ("lig_active", P),
-                ("prop_tries", I)]
+                ("prop_tries", I), ("hint", P)]
 
 
 SP = ctypes.POINTER
@@ -77,7 +77,8 @@ _SIGS = {
     "adock_rescore64": ([SP(Ligands), SP(Work), SP(Grids), SP(SF), SP(Receptors), P, I, P, P, P, P, P], I),
     "adock_mc_noalloc_scratch_bytes": ([I, I, I, I], ctypes.c_size_t),
     "adock_mc_noalloc": ([SP(Ligands), SP(Grids), SP(SF), SP(Receptors), SP(McArgs), P], I),
-    "adock_prop_features": ([SP(Ligands), SP(Work), SP(Grids), SP(SF), P, I, P, P, P], I),
+    "adock_prop_features": ([SP(Ligands), SP(Work), SP(Grids), SP(SF), P, I, P, P, P, P, P], I),
+    "adock_prop_hint": ([I, I, P, P, I, P, P, P, P], I),
     "adock_prop_sample": ([SP(Ligands), SP(Work), P, P, I, P, P, I, I, ctypes.c_ulonglong, I, P, P], I),
     "adock_gemm_bf16": ([I, I, I, P, ctypes.c_longlong, ctypes.c_longlong, P, ctypes.c_longlong, ctypes.c_longlong, P,
                          ctypes.c_longlong, F, P, I, P, P, ctypes.c_longlong, P], I),

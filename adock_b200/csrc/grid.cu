@@ -23,6 +23,11 @@ namespace adock {
 #define TILE_Z 8
 #define TILE_THREADS 128
 #define STAGE_CAP 2048
+// The fitted kernel stages fewer atoms per pass: its per-block weight slice (receptor types x 8 ligand types x 6
+// basis weights, 21 KB for the 108 receptor ext types) and 896 staged atoms (14 KB) fit 6 blocks per SM; at the
+// 2,048 of the Vina kernel only 4 fit. A tile's cutoff region holds a few hundred atoms at protein density, so
+// one pass still covers it.
+#define FIT_STAGE_CAP 896
 #define VINA_GROUP 8
 #define FIT_GROUP 8
 #define MAX_COLUMNS 64
@@ -85,8 +90,10 @@ __device__ int tile_columns(const Cells& C, int n_rec, const float* lo, const fl
     return begin[MAX_COLUMNS];
 }
 
-// Stage the atoms inside [lo, hi] (per axis) from position `start` of the concatenated columns; returns the
-// position where staging stopped (the total when all atoms were seen). Staged order = column order.
+// Stage the atoms inside [lo, hi] (per axis) from position `start` of the concatenated columns, at most CAP
+// (a multiple of TILE_THREADS); returns the position where staging stopped (the total when all atoms were seen).
+// Staged order = column order.
+template <int CAP>
 __device__ __forceinline__ int stage_atoms(const float* __restrict__ rxyz, const int* __restrict__ rtype,
                                            const int* begin, const int* off, int ncol, int start, const float* lo,
                                            const float* hi, float4* S, int* count, int* wsum) {
@@ -95,7 +102,7 @@ __device__ __forceinline__ int stage_atoms(const float* __restrict__ rxyz, const
     int n = 0;
     int v0 = start;
     for (; v0 < total; v0 += TILE_THREADS) {
-        if (n + TILE_THREADS > STAGE_CAP) break;
+        if (n + TILE_THREADS > CAP) break;
         const int v = v0 + tid;
         bool in = false;
         float x = 0.f, y = 0.f, z = 0.f;
@@ -188,7 +195,7 @@ __global__ void __launch_bounds__(TILE_THREADS) grid_vina_kernel(const float* __
         const int total = col_off[ncol];
         while (start < total) {
             int cnt;
-            start = stage_atoms(rxyz, rtype, col_begin, col_off, ncol, start, lo, hi, S, &cnt, wsum);
+            start = stage_atoms<STAGE_CAP>(rxyz, rtype, col_begin, col_off, ncol, start, lo, hi, S, &cnt, wsum);
             if (valid) {
                 for (int s = 0; s < cnt; ++s) {
                     const float4 A = S[s];
@@ -240,7 +247,7 @@ __global__ void __launch_bounds__(TILE_THREADS) grid_fit_kernel(const float* __r
                                                                 const __grid_constant__ FitPrm P,
                                                                 const float* __restrict__ W, const float* __restrict__ rad_rec,
                                                                 float* __restrict__ out) {
-    __shared__ float4 S[STAGE_CAP];
+    __shared__ float4 S[FIT_STAGE_CAP];
     __shared__ int wsum[TILE_THREADS / 32];
     extern __shared__ float Wsh[];   // [n_rt, FIT_GROUP, 6] slice of W (radius-ordered types), then rad_rec [n_rt]
     float* Rsh = Wsh + (size_t)P.n_rt * FIT_GROUP * 6;
@@ -267,7 +274,7 @@ __global__ void __launch_bounds__(TILE_THREADS) grid_fit_kernel(const float* __r
         const int total = col_off[ncol];
         while (start < total) {
             int cnt;
-            start = stage_atoms(rxyz, rext, col_begin, col_off, ncol, start, lo, hi, S, &cnt, wsum);
+            start = stage_atoms<FIT_STAGE_CAP>(rxyz, rext, col_begin, col_off, ncol, start, lo, hi, S, &cnt, wsum);
             if (valid) {
                 for (int s = 0; s < cnt; ++s) {
                     const float4 A = S[s];

@@ -362,6 +362,7 @@ extern "C" int adock_mc(const adock_ligands_t* lig, const adock_work_t* work, co
     M.prop_frac = (mc->prop_frac <= 0.f || mc->prop_frac >= 1.f) ? 1.f : mc->prop_frac;
     M.log_x = (__nv_bfloat16*)mc->log_x; M.log_y = mc->log_y; M.log_n = mc->log_n; M.log_cap = mc->log_cap;
     M.lig_active = mc->lig_active;
+    M.hint = mc->hint;
     M.prop_tries = mc->prop_tries > 1 ? mc->prop_tries : 1;
     ADOCK_CHECK_ARG(!mc->prop || mc->prop_k % M.prop_tries == 0, "prop_k must be a multiple of prop_tries");
     const TypeTables tt = make_tables(sf);
@@ -531,8 +532,8 @@ extern "C" int adock_mc_noalloc(const adock_ligands_t* lig, const adock_grids_t*
 
 // ------------------------------------------------------------------------------------------ proposal entry points
 extern "C" int adock_prop_features(const adock_ligands_t* lig, const adock_work_t* work, const adock_grids_t* grids,
-                                   const adock_sf_t* sf, const int* chain_lig, int n, const float* state, void* feat,
-                                   void* stream) {
+                                   const adock_sf_t* sf, const int* chain_lig, int n, const float* state,
+                                   const float* cur_e, const float* hint, void* feat, void* stream) {
     SearchParams P;
     int rc = make_params(P, lig, work, grids, sf, nullptr);
     if (rc) return rc;
@@ -543,11 +544,70 @@ extern "C" int adock_prop_features(const adock_ligands_t* lig, const adock_work_
     cudaStream_t st = (cudaStream_t)stream;
     __nv_bfloat16* out = (__nv_bfloat16*)feat;
     switch (grids->dtype) {
-        case ADOCK_GRID_F32: return launch_prop_features<float>(P, chain_lig, n, state, out, st);
-        case ADOCK_GRID_F16: return launch_prop_features<__half>(P, chain_lig, n, state, out, st);
-        case ADOCK_GRID_BF16: return launch_prop_features<__nv_bfloat16>(P, chain_lig, n, state, out, st);
+        case ADOCK_GRID_F32: return launch_prop_features<float>(P, chain_lig, n, state, cur_e, hint, out, st);
+        case ADOCK_GRID_F16: return launch_prop_features<__half>(P, chain_lig, n, state, cur_e, hint, out, st);
+        case ADOCK_GRID_BF16:
+            return launch_prop_features<__nv_bfloat16>(P, chain_lig, n, state, cur_e, hint, out, st);
     }
     ADOCK_CHECK_ARG(false, "unknown grid dtype %d", grids->dtype);
+}
+
+// Ligand-best rows of the proposal features. Pass 1 reduces, per ligand, the key (order-preserving bits of the
+// chain's best energy << 32 | chain index) with atomicMin, so ties go to the lowest chain index and non-finite
+// energies never win; pass 2 copies the winning chain's best state (t, q, torsions 0..19), its energy and a valid
+// flag into hint[l].
+namespace adock {
+__device__ __forceinline__ unsigned long long energy_key(float e, int ch) {
+    const unsigned u = __float_as_uint(e);
+    const unsigned o = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+    return ((unsigned long long)o << 32) | (unsigned)ch;
+}
+
+__global__ void prop_hint_reduce_kernel(int n, const int* chain_lig, const float* best_e, int L,
+                                        unsigned long long* keys) {
+    const int ch = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ch >= n) return;
+    const int l = chain_lig[ch];
+    const float e = best_e[ch];
+    if (l < 0 || l >= L || !isfinite(e)) return;
+    atomicMin(keys + l, energy_key(e, ch));
+}
+
+__global__ void prop_hint_copy_kernel(int L, const unsigned long long* keys, const float* best, int SD,
+                                      const float* best_e, float* hint) {
+    const int l = blockIdx.x;
+    const unsigned long long key = keys[l];
+    const bool ok = key != ~0ull;
+    const int ch = (int)(key & 0xffffffffull);
+    float* h = hint + (long long)l * PROP_HINT;
+    for (int i = threadIdx.x; i < PROP_HINT; i += blockDim.x) {
+        float v = 0.f;
+        if (ok) {
+            if (i < 27 && i < SD) v = best[(long long)ch * SD + i];
+            else if (i == 27) v = best_e[ch];
+            else if (i == 28) v = 1.f;
+        }
+        h[i] = v;
+    }
+}
+}  // namespace adock
+
+extern "C" int adock_prop_hint(int L, int n, const int* chain_lig, const float* best, int SD, const float* best_e,
+                               void* keys, float* hint, void* stream) {
+    ADOCK_CHECK_ARG(L >= 0 && n >= 0, "negative size");
+    ADOCK_CHECK_ARG(SD >= 7, "SD must be >= 7");
+    if (L == 0) return ADOCK_OK;
+    ADOCK_CHECK_ARG(keys && hint && (n == 0 || (chain_lig && best && best_e)), "null array argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    ADOCK_CUDA(cudaMemsetAsync(keys, 0xff, (size_t)L * sizeof(unsigned long long), st));
+    if (n > 0) {
+        prop_hint_reduce_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, chain_lig, best_e, L,
+                                                                            (unsigned long long*)keys);
+        ADOCK_CUDA(cudaGetLastError());
+    }
+    prop_hint_copy_kernel<<<(unsigned)L, 32, 0, st>>>(L, (const unsigned long long*)keys, best, SD, best_e, hint);
+    ADOCK_CUDA(cudaGetLastError());
+    return ADOCK_OK;
 }
 
 extern "C" int adock_prop_sample(const adock_ligands_t* lig, const adock_work_t* work, const int* chain_lig,

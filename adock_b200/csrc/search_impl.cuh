@@ -83,16 +83,18 @@ struct McParams {
     int prop_k;
     float prop_frac;                 // fraction of steps that take the learned move (the rest: plain MC)
     unsigned long long* prop_stats;  // [4] proposals made, proposals accepted, plain steps, plain accepted
-    // training-data log of accepted improving moves: features [cap, 288] BF16, moves [cap, 32]
+    // training-data log of accepted improving moves: features [cap, 320] BF16, moves [cap, 32]
     __nv_bfloat16* log_x;
     float* log_y;
     int* log_n;
     int log_cap;
     const int* lig_active;           // [L] or NULL: chains of a ligand with flag 0 are left unchanged
     int prop_tries;                  // learned steps: candidate targets per step (the lowest-energy one is optimised)
+    const float* hint;               // [L, PROP_HINT] ligand-best rows for the logged features, or NULL
 };
 
-#define PROP_IN 288
+#define PROP_IN 320
+#define PROP_HINT 32
 #define PROP_MOVE 32
 #define PROP_FAIL_MAX 8
 
@@ -595,7 +597,10 @@ __device__ ADOCK_BFGS_ATTR float bfgs(float* ws, const WSLayout& L, float* x, in
 }
 
 // ------------------------------------------------------------------------------------------ proposal features
-// Feature row (288 values, BF16) of state s of ligand l, computed by one warp:
+// sign(v) log(1 + |v|): energies and map values of any magnitude in a range the network handles
+__device__ __forceinline__ float slog(float v) { return copysignf(log1pf(fabsf(v)), v); }
+
+// Feature row (PROP_IN = 320 values, BF16) of state s (energy e) of ligand l, computed by one warp:
 //   [0, 216)   27 samples x 8 maps: nearest-grid map values at the centroid + {-2, 0, 2} A per axis, as
 //              sign(v) log(1 + |v|) (maps beyond the receptor's count are 0)
 //   [216, 219) translation relative to the box centre / 10 A
@@ -603,10 +608,19 @@ __device__ ADOCK_BFGS_ATTR float bfgs(float* ws, const WSLayout& L, float* x, in
 //   [223, 263) sin, cos of torsions 0..19 (0 beyond the ligand's torsion count)
 //   [263, 275) heavy atoms / 64, torsions / 20, radius of gyration / 10, intra pairs / 2000, fraction of atoms
 //              per map slot 0..7
-//   [275, 288) 0
+//   ligand-best hint (hint: the lowest-energy state over the ligand's chains, PROP_HINT floats = t, q, torsions
+//   0..19, energy at 27, valid flag at 28; all 0 when hint is NULL or not valid):
+//   [275, 278) (t_hint - t) / 10 A
+//   [278, 281) rotation vector of q_hint q^-1 (w >= 0) / pi
+//   [281]      slog(e - e_hint)
+//   [282]      slog(e) (0 when e is not finite)
+//   [283]      1
+//   [284, 288) 0
+//   [288, 308) torsion differences theta_hint - theta wrapped to [-pi, pi), / pi (0 beyond the torsion count)
+//   [308, 320) 0
 template <typename GT>
-__device__ ADOCK_COLD_ATTR void prop_features(const SearchParams& P, int l, const float* s, __nv_bfloat16* out,
-                                              int lane) {
+__device__ ADOCK_COLD_ATTR void prop_features(const SearchParams& P, int l, const float* s, float e, const float* hint,
+                                              __nv_bfloat16* out, int lane) {
     const int4 inf = P.info[l];
     const int na = inf.x, nt = inf.y, np = inf.z, ri = inf.w;
     const int nx = (int)P.dims[3 * ri], ny = (int)P.dims[3 * ri + 1], nz = (int)P.dims[3 * ri + 2];
@@ -622,7 +636,7 @@ __device__ ADOCK_COLD_ATTR void prop_features(const SearchParams& P, int l, cons
         const long long idx = ((long long)i * ny + j) * nz + k;
         for (int q = 0; q < 8; ++q) {
             const float v = q < nm ? gload(G + q * n3 + idx) : 0.f;
-            out[lane * 8 + q] = __float2bfloat16(copysignf(log1pf(fabsf(v)), v));
+            out[lane * 8 + q] = __float2bfloat16(slog(v));
         }
     }
     if (lane == 27) {
@@ -647,7 +661,42 @@ __device__ ADOCK_COLD_ATTR void prop_features(const SearchParams& P, int l, cons
         for (int a = 0; a < na; ++a) cnt += ((__float_as_int(P.atoms[(long long)l * P.AM + a].w) & 0xffff) == q);
         out[267 + q] = __float2bfloat16(na ? (float)cnt / na : 0.f);
     }
-    if (lane < 13) out[275 + lane] = __float2bfloat16(0.f);
+    // ligand-best hint
+    const bool hv = hint != nullptr && hint[28] > 0.5f;
+    if (lane == 0) {
+        float f[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (hv) {
+            for (int d = 0; d < 3; ++d) f[d] = (hint[d] - s[d]) * 0.1f;
+            // r = q_hint * conj(q), both normalised; rotation vector 2 atan2(|v|, w) v / |v|
+            const float na = rsqrtf(s[3] * s[3] + s[4] * s[4] + s[5] * s[5] + s[6] * s[6]);
+            const float nb = rsqrtf(hint[3] * hint[3] + hint[4] * hint[4] + hint[5] * hint[5] + hint[6] * hint[6]);
+            const float aw = s[3] * na, ax = -s[4] * na, ay = -s[5] * na, az = -s[6] * na;
+            const float bw = hint[3] * nb, bx = hint[4] * nb, by = hint[5] * nb, bz = hint[6] * nb;
+            float rw = bw * aw - bx * ax - by * ay - bz * az;
+            float rx = bw * ax + bx * aw + by * az - bz * ay;
+            float ry = bw * ay - bx * az + by * aw + bz * ax;
+            float rz = bw * az + bx * ay - by * ax + bz * aw;
+            if (rw < 0.f) { rw = -rw; rx = -rx; ry = -ry; rz = -rz; }
+            const float sn = sqrtf(rx * rx + ry * ry + rz * rz);
+            const float sc = sn > 1e-7f ? 2.f * atan2f(sn, rw) / sn : 2.f;
+            f[3] = rx * sc * 0.31830988f; f[4] = ry * sc * 0.31830988f; f[5] = rz * sc * 0.31830988f;
+            f[6] = isfinite(e) ? slog(e - hint[27]) : 0.f;
+            f[8] = 1.f;
+        }
+        f[7] = (hv && isfinite(e)) ? slog(e) : 0.f;
+        for (int i = 0; i < 9; ++i) out[275 + i] = __float2bfloat16(isfinite(f[i]) ? f[i] : 0.f);
+        for (int i = 284; i < 288; ++i) out[i] = __float2bfloat16(0.f);
+    }
+    if (lane < 20) {
+        float d = 0.f;
+        if (hv && lane < nt) {
+            d = hint[7 + lane] - s[7 + lane];
+            d = d - 6.2831853f * floorf((d + 3.14159265f) * 0.15915494f);
+            d = isfinite(d) ? d * 0.31830988f : 0.f;
+        }
+        out[288 + lane] = __float2bfloat16(d);
+    }
+    if (lane < 12) out[308 + lane] = __float2bfloat16(0.f);
     __syncwarp();
 }
 
@@ -780,7 +829,8 @@ __global__ void __launch_bounds__(128, MINB) mc_kernel(const __grid_constant__ S
                 if (lane == 0) row = atomicAdd(M.log_n, 1);
                 row = __shfl_sync(0xffffffffu, row, 0);
                 if (row < M.log_cap) {
-                    prop_features<GT>(P, l, cur, M.log_x + (long long)row * PROP_IN, lane);
+                    prop_features<GT>(P, l, cur, ec, M.hint ? M.hint + (long long)l * PROP_HINT : nullptr,
+                                      M.log_x + (long long)row * PROP_IN, lane);
                     if (lane == 0) log_state(cur, c.nt, ch, M.log_y + (long long)row * PROP_MOVE);
                 }
                 __syncwarp();
@@ -1043,10 +1093,11 @@ __global__ void __launch_bounds__(128) rescore64_kernel(const __grid_constant__ 
     }
 }
 
-// feature rows of n states (one warp per state)
+// feature rows of n states (one warp per state); cur_e [n] and hint [L, PROP_HINT] may be NULL
 template <typename GT>
 __global__ void __launch_bounds__(128) prop_features_kernel(const __grid_constant__ SearchParams P, const int* chain_lig,
-                                                            int n, const float* state, __nv_bfloat16* out) {
+                                                            int n, const float* state, const float* cur_e,
+                                                            const float* hint, __nv_bfloat16* out) {
     __shared__ float s[4][7 + 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int ch = blockIdx.x * 4 + wid;
@@ -1054,7 +1105,9 @@ __global__ void __launch_bounds__(128) prop_features_kernel(const __grid_constan
     const int SDM = 7 + P.KM;
     for (int i = lane; i < SDM && i < 7 + 32; i += 32) s[wid][i] = state[(long long)ch * SDM + i];
     __syncwarp();
-    prop_features<GT>(P, chain_lig[ch], s[wid], out + (long long)ch * PROP_IN, lane);
+    const int l = chain_lig[ch];
+    prop_features<GT>(P, l, s[wid], cur_e ? cur_e[ch] : 0.f, hint ? hint + (long long)l * PROP_HINT : nullptr,
+                      out + (long long)ch * PROP_IN, lane);
 }
 
 // ------------------------------------------------------------------------------------------ launchers
@@ -1151,16 +1204,16 @@ int launch_rescore64(const SearchParams& P, const int* cl, int n, const float* s
 }
 
 template <typename GT>
-int launch_prop_features(const SearchParams& P, const int* cl, int n, const float* state, __nv_bfloat16* out,
-                         cudaStream_t st) {
-    prop_features_kernel<GT><<<(unsigned)((n + 3) / 4), 128, 0, st>>>(P, cl, n, state, out);
+int launch_prop_features(const SearchParams& P, const int* cl, int n, const float* state, const float* cur_e,
+                         const float* hint, __nv_bfloat16* out, cudaStream_t st) {
+    prop_features_kernel<GT><<<(unsigned)((n + 3) / 4), 128, 0, st>>>(P, cl, n, state, cur_e, hint, out);
     ADOCK_CUDA(cudaGetLastError());
     return ADOCK_OK;
 }
 
 #define ADOCK_SEARCH_INSTANTIATE(GT)                                                                              \
-    template int launch_prop_features<GT>(const SearchParams&, const int*, int, const float*, __nv_bfloat16*,     \
-                                          cudaStream_t);                                                          \
+    template int launch_prop_features<GT>(const SearchParams&, const int*, int, const float*, const float*,       \
+                                          const float*, __nv_bfloat16*, cudaStream_t);                            \
     template int launch_mc<GT>(const SearchParams&, const McParams&, const TypeTables&, cudaStream_t, int);       \
     template int launch_eg<GT>(const SearchParams&, const int*, int, const float*, float*, float*, int,           \
                                const TypeTables&, cudaStream_t);                                                  \
@@ -1171,8 +1224,8 @@ int launch_prop_features(const SearchParams& P, const int* cl, int n, const floa
                                       float*, const TypeTables&, const adock_sf_t&, cudaStream_t);
 
 #define ADOCK_SEARCH_EXTERN(GT)                                                                                   \
-    extern template int launch_prop_features<GT>(const SearchParams&, const int*, int, const float*,              \
-                                                 __nv_bfloat16*, cudaStream_t);                                   \
+    extern template int launch_prop_features<GT>(const SearchParams&, const int*, int, const float*, const float*, \
+                                                 const float*, __nv_bfloat16*, cudaStream_t);                     \
     extern template int launch_mc<GT>(const SearchParams&, const McParams&, const TypeTables&, cudaStream_t, int); \
     extern template int launch_eg<GT>(const SearchParams&, const int*, int, const float*, float*, float*, int,    \
                                       const TypeTables&, cudaStream_t);                                           \

@@ -141,16 +141,34 @@ class B200KernelProblem:
         self.mc_variant = tune_mc(self, self._i32(chain_lig), state.contiguous())
         return self.mc_variant
 
-    def prop_features(self, chain_lig, state):
-        """Proposal-network feature rows [N, 288] (BF16) of N states."""
+    def prop_features(self, chain_lig, state, cur_e=None, hint=None):
+        """Proposal-network feature rows [N, 320] (BF16) of N states; with the states' energies cur_e [N] and the
+        ligand-best rows hint [L, 32] (prop_hint) the ligand-best columns are filled, else they are 0."""
         N = state.shape[0]
-        out = torch.empty(N, 288, dtype=torch.bfloat16, device=self.device)
+        out = torch.empty(N, 320, dtype=torch.bfloat16, device=self.device)
         cl = self._i32(chain_lig)
         st = state.to(self.device, torch.float32).contiguous()
+        ce = None if cur_e is None else cur_e.to(self.device, torch.float32).contiguous()
+        if hint is not None:
+            assert hint.shape == (self.L, 32) and hint.dtype == torch.float32 and hint.is_contiguous()
         with torch.cuda.device(self.device):
             _lib.call("adock_prop_features", self.c_lig, self.c_work, self.c_grids, self.c_sf, _lib.ptr(cl), N,
-                      _lib.ptr(st), _lib.ptr(out), _lib.stream_ptr())
+                      _lib.ptr(st), _lib.ptr(ce), _lib.ptr(hint), _lib.ptr(out), _lib.stream_ptr())
         return out
+
+    def prop_hint(self, chain_lig, best, best_e):
+        """Ligand-best rows [L, 32]: per ligand, the best state (t, q, torsions 0..19) of its chain with the lowest
+        finite best energy, that energy (column 27) and a valid flag (column 28); zeros for a ligand without one."""
+        N = best.shape[0]
+        hint = torch.empty(self.L, 32, device=self.device)
+        keys = torch.empty(self.L, dtype=torch.int64, device=self.device)
+        cl = self._i32(chain_lig)
+        b = best.float().contiguous()
+        be = best_e.float().contiguous()
+        with torch.cuda.device(self.device):
+            _lib.call("adock_prop_hint", self.L, N, _lib.ptr(cl), _lib.ptr(b), int(b.shape[1]), _lib.ptr(be),
+                      _lib.ptr(keys), _lib.ptr(hint), _lib.stream_ptr())
+        return hint
 
     def prop_sample(self, chain_lig, chain_id, net_out, state, k, seed, segment):
         """Target states [N, k, 32] (t, q, torsions 0..19) drawn from the network's Gaussian (net_out [N, 64]) over
@@ -169,15 +187,16 @@ class B200KernelProblem:
 
     def run_mc(self, chain_lig, chain_id, cur, cur_e, best, best_e, init_opt, mc_steps, bfgs_iters, temp,
                amp_pos, amp_rot, seed, step_offset, exact=False, nbr=None, nbr_n=None, order=None, variant=None,
-               prop=None, prop_stats=None, log=None, prop_frac=1.0, lig_active=None, prop_tries=1):
+               prop=None, prop_stats=None, log=None, prop_frac=1.0, lig_active=None, prop_tries=1, hint=None):
         """In place on cur/cur_e/best/best_e (float32 contiguous CUDA tensors). exact=True with nbr [N, NB] int32 /
         nbr_n [N]: each chain's exact inter energy loops only over its receptor-atom neighbour list.
         variant: MC launch variant (default: the tuned one, else the library default).
         prop: learned moves [N, k, 32] for steps 0..k-1 of this launch (plain MC fallback after 8 rejections);
-        prop_stats: int64 [4] counters; log: (x BF16 [cap, 288], y [cap, 32], n int32 [1]) training-data log;
+        prop_stats: int64 [4] counters; log: (x BF16 [cap, 320], y [cap, 32], n int32 [1]) training-data log;
         prop_frac: fraction of steps that take the learned move (the others take the plain random move);
         lig_active: int32 [L] device flags, chains of ligands with 0 are left unchanged (None: all run);
-        prop_tries: candidate targets per learned step (prop then holds steps x prop_tries targets per chain)."""
+        prop_tries: candidate targets per learned step (prop then holds steps x prop_tries targets per chain);
+        hint: ligand-best rows [L, 32] (prop_hint) for the logged features (None: those columns are 0)."""
         N = cur.shape[0]
         if N == 0:
             return
@@ -220,6 +239,10 @@ class B200KernelProblem:
             assert lig_active.dtype == torch.int32 and lig_active.is_contiguous() and lig_active.numel() == self.L
             a.lig_active = _lib.ptr(lig_active)
             keep.append(lig_active)
+        if hint is not None:
+            assert hint.shape == (self.L, 32) and hint.dtype == torch.float32 and hint.is_contiguous()
+            a.hint = _lib.ptr(hint)
+            keep.append(hint)
         with torch.cuda.device(self.device):
             _lib.call("adock_mc", self.c_lig, self.c_work, self.c_grids, self.c_sf, self.c_rec, a, _lib.stream_ptr())
         self._keep_mc = keep

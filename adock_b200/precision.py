@@ -33,16 +33,19 @@ def random_poses(prob, kp, n_poses, seed=0, sigma=1.5):
     return cl, kp.pack(t, q, th)
 
 
-def _time(fn, reps=3):
-    fn()
+def _time(fn, reps=10, warmup=2):
+    """(last output, median ms per call): each call bracketed by its own events, so a one-off host delay (an
+    allocation, a module load) in one call does not enter the figure."""
+    for _ in range(warmup):
+        fn()
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(reps):
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+    for e0, e1 in ev:
+        e0.record()
         out = fn()
-    e1.record()
+        e1.record()
     torch.cuda.synchronize()
-    return out, e0.elapsed_time(e1) / reps
+    return out, float(np.median([e0.elapsed_time(e1) for e0, e1 in ev]))
 
 
 def precision_report(rec, ligs, n_poses=100_000, device="cuda", dtypes=("f32", "f16", "bf16"), seed=0):

@@ -1,6 +1,6 @@
 """Learned Monte-Carlo proposal (no reference counterpart).
 
-A small MLP proposes the MC move of each chain: x [288 features of the chain's current state] -> SiLU(256) ->
+A small MLP proposes the MC move of each chain: x [320 features of the chain's current state] -> SiLU(256) ->
 SiLU(256) -> 64 outputs = Gaussian means (columns 0..25) and log standard deviations (32..57) of the move
 (translation 3 A, rotation vector 3 rad, torsion deltas 20 rad). Weights are BF16 on the tensor cores with FP32
 accumulation; training keeps FP32 master weights and Adam moments. Every kernel is the library's own
@@ -12,6 +12,10 @@ state to the chain's best state at the end of the run. In the search (``run_mc_s
 steps take the network's move instead of the random perturbation (the sampled spread has floors so the moves keep
 exploring); the Vina-form energy with BFGS and the Metropolis test still decide every move, and a chain whose
 learned moves are rejected 8 times in a row falls back to plain MC until it accepts a move.
+
+A network with ``uses_hint`` also reads the ligand-best hint: before each segment, the best state over the chain's
+ligand's chains (``B200KernelProblem.prop_hint``), given relative to the chain's state (translation, rotation and
+torsion differences, energy difference). Without it those columns (``HINT_COLS``) are 0, in training and search.
 """
 from __future__ import annotations
 
@@ -22,7 +26,8 @@ import torch
 
 from . import _lib
 
-IN, HID, OUT = 288, 256, 64
+IN, HID, OUT = 320, 256, 64
+HINT_COLS = list(range(275, 284)) + list(range(288, 308))   # ligand-best hint columns of the feature row
 
 
 def _gemm(A, sA, B, sB, M, N, K, C=None, beta=0.0, bias=None, act=0, pre=None, Cb=None):
@@ -40,9 +45,10 @@ def check_gemm(where):
 
 
 class ProposalNet:
-    """288 -> 256 -> 256 -> 64 MLP; weights W_i stored [K, N] row-major (x @ W)."""
+    """320 -> 256 -> 256 -> 64 MLP; weights W_i stored [K, N] row-major (x @ W). uses_hint: the network reads the
+    ligand-best hint columns (else they are 0 in its inputs)."""
 
-    def __init__(self, device="cuda", seed=0, init_log_sd=(0.0, -1.0, -0.5)):
+    def __init__(self, device="cuda", seed=0, init_log_sd=(0.0, -1.0, -0.5), uses_hint=False):
         dev = torch.device(device)
         g = torch.Generator(device="cpu").manual_seed(seed)
         dims = [(IN, HID), (HID, HID), (HID, OUT)]
@@ -59,18 +65,21 @@ class ProposalNet:
         self.v = [torch.zeros_like(p) for p in self.params]
         self.step = 0
         self.device = dev
+        self.uses_hint = bool(uses_hint)
 
     def state_dict(self):
-        return {"W": [w.cpu() for w in self.W], "b": [b.cpu() for b in self.b], "step": self.step}
+        return {"W": [w.cpu() for w in self.W], "b": [b.cpu() for b in self.b], "step": self.step,
+                "uses_hint": self.uses_hint}
 
     def load_state_dict(self, d):
         for dst, src in zip(self.W + self.b, d["W"] + d["b"]):
             dst.copy_(src.to(self.device))
         self.Wb = [w.to(torch.bfloat16).contiguous() for w in self.W]
         self.step = int(d.get("step", 0))
+        self.uses_hint = bool(d.get("uses_hint", False))
 
     def forward(self, x, save=False):
-        """x: BF16 [B, 288] -> out FP32 [B, 64] (and saved activations when save)."""
+        """x: BF16 [B, 320] -> out FP32 [B, 64] (and saved activations when save)."""
         B = x.shape[0]
         dev = self.device
         pre1 = torch.empty(B, HID, device=dev)
@@ -130,7 +139,7 @@ class ProposalNet:
         return loss
 
     def fit(self, X, Y, epochs=3, batch=4096, lr=1e-3, seed=0, log=None):
-        """Minibatch Adam over (X BF16 [n, 288], Y [n, 32]); returns the mean loss of the last epoch."""
+        """Minibatch Adam over (X BF16 [n, 320], Y [n, 32]); returns the mean loss of the last epoch."""
         n = X.shape[0]
         g = torch.Generator(device=self.device).manual_seed(seed)
         last = float("nan")
@@ -190,18 +199,34 @@ def ligand_best_chain(chain_lig, best_e):
     return torch.full((L,), -1, dtype=torch.long, device=best_e.device).scatter_reduce(0, lig, cand, "amax")
 
 
-def collect(kp, chain_lig, chain_id, cur, cur_e, best, best_e, cfg, seed, cap, init_opt=True, target="chain"):
-    """Run the plain MC search on the given chains with the training-data log on; returns (X BF16 [n, 288],
+def without_hint(X):
+    """Feature rows with the ligand-best hint columns set to 0 (the inputs of a network without the hint)."""
+    X = X.clone()
+    X[:, HINT_COLS] = 0
+    return X
+
+
+def collect(kp, chain_lig, chain_id, cur, cur_e, best, best_e, cfg, seed, cap, init_opt=True, target="chain",
+            hint_segment=0):
+    """Run the plain MC search on the given chains with the training-data log on; returns (X BF16 [n, 320],
     Y [n, 32]): the features of the pre-move state of each accepted improving move and, as its target, the move
     from that state to a low-energy minimum the run found (n <= cap). target "chain": the chain's own best state
     at the end of the run; "ligand": the best state over all chains of the chain's ligand; "both": returns
-    (X, Y_chain, Y_ligand)."""
+    (X, Y_chain, Y_ligand). hint_segment > 0: the run is cut into launches of that many steps (the same moves:
+    the random streams are indexed by step) and the logged features carry the ligand-best hint taken before each
+    launch; 0: one launch, hint columns 0."""
     dev = kp.device
     lx = torch.empty(cap, IN, dtype=torch.bfloat16, device=dev)
     ly = torch.empty(cap, 32, device=dev)
     ln = torch.zeros(1, dtype=torch.int32, device=dev)
-    kp.run_mc(chain_lig, chain_id, cur, cur_e, best, best_e, init_opt, cfg["mc_steps"], cfg["bfgs_iters"],
-              cfg["mc_temperature"], cfg["mc_amp_pos"], cfg["mc_amp_rot"], seed, 0, log=(lx, ly, ln))
+    steps = cfg["mc_steps"]
+    seg = hint_segment if hint_segment > 0 else max(steps, 1)
+    for sg in range(max(1, math.ceil(steps / seg))):
+        k = min(seg, steps - sg * seg)
+        hint = kp.prop_hint(chain_lig, best, best_e) if hint_segment > 0 and sg > 0 else None
+        kp.run_mc(chain_lig, chain_id, cur, cur_e, best, best_e, init_opt and sg == 0, k, cfg["bfgs_iters"],
+                  cfg["mc_temperature"], cfg["mc_amp_pos"], cfg["mc_amp_rot"], seed, sg * seg, log=(lx, ly, ln),
+                  hint=hint)
     n = min(int(ln), cap)
     states = ly[:n]
     ch = states[:, 28].long()
@@ -227,7 +252,7 @@ def _finite_rows(X, ok, *Ys):
     return keep
 
 
-def collect_learned(kp, net, chain_lig, chain_id, cur, cfg, seed, cap, prop_k=32, prop_frac=0.3):
+def collect_learned(kp, net, chain_lig, chain_id, cur, cfg, seed, cap, prop_k=32, prop_frac=0.3, prop_tries=1):
     """The learned search (``run_mc_segments`` with ``net``) from the states ``cur`` with the training-data log on;
     returns (X, Y) as ``collect`` does, the targets being the learned search's own final minima of each chain."""
     dev = kp.device
@@ -238,7 +263,7 @@ def collect_learned(kp, net, chain_lig, chain_id, cur, cfg, seed, cap, prop_k=32
     ly = torch.empty(cap, 32, device=dev)
     ln = torch.zeros(1, dtype=torch.int32, device=dev)
     run_mc_segments(kp, net, chain_lig, chain_id, cur, ce, best, be, cfg, seed, prop_k=prop_k, prop_frac=prop_frac,
-                    log=(lx, ly, ln))
+                    log=(lx, ly, ln), prop_tries=prop_tries)
     n = min(int(ln), cap)
     states = ly[:n]
     tgt = best[states[:, 28].long()]
@@ -306,10 +331,15 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
     best = cur.clone()
     ce, be = torch.zeros(N, device=dev), torch.full((N,), float("inf"), device=dev)
     torch.cuda.synchronize(dev)
-    # learned variants: (name, segment steps, learned fraction[, training "chain" | "ligand" | "dagger"]): the
-    # chain's or the ligand's best pose as target, or the chain network fine-tuned on its own search's moves
-    variants = {v[0]: (v[1], v[2], v[3] if len(v) > 3 else "chain", int(v[4]) if len(v) > 4 else 1) for v in learned}
-    X, Yc, Yl = collect(kp_t, cl, ci, cur, ce, best, be, cfg_tr, seed=seed + 1, cap=log_cap, target="both")
+    # learned variants: (name, segment steps, learned fraction[, training "chain" | "ligand" | "dagger" |
+    # "daggerN"[, tries[, hint]]]): the chain's or the ligand's best pose as target, or the chain network
+    # fine-tuned N times on its own search's moves; tries candidate targets per learned step; hint: the network
+    # reads the ligand-best hint
+    variants = {v[0]: (v[1], v[2], v[3] if len(v) > 3 else "chain", int(v[4]) if len(v) > 4 else 1,
+                       bool(v[5]) if len(v) > 5 else False) for v in learned}
+    any_hint = any(h for (_, _, _, _, h) in variants.values())
+    X, Yc, Yl = collect(kp_t, cl, ci, cur, ce, best, be, cfg_tr, seed=seed + 1, cap=log_cap, target="both",
+                        hint_segment=32 if any_hint else 0)
     nets = {}
     out["train"] = {"moves": int(X.shape[0]), "epochs": epochs}
     def rounds(t):   # "dagger" = 1 self-training round on top of "chain", "dagger2" = 2, ...
@@ -318,32 +348,33 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
     def dagger_name(n):
         return "chain" if n == 0 else ("dagger" if n == 1 else f"dagger{n}")
 
-    targets = {t for (_, _, t, _) in variants.values()}
-    for n in range(max(rounds(t) for t in targets)):
-        targets.add(dagger_name(n))
-    for tgt in sorted(targets, key=lambda t: (t == "ligand", rounds(t))):
+    targets = {(t, h) for (_, _, t, _, h) in variants.values()}
+    for (t, h) in list(targets):
+        for n in range(rounds(t)):
+            targets.add((dagger_name(n), h))
+    for (tgt, hint) in sorted(targets, key=lambda th: (th[1], th[0] == "ligand", rounds(th[0]))):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         n = rounds(tgt)
         if n > 0:
             # self-training round n: the previous round's network drives the search on the training ligands with
             # the log on; a copy of it is fine-tuned on those moves (targets: that search's own final minima)
-            prev = nets[dagger_name(n - 1)]
-            net = ProposalNet(dev, seed=seed)
+            prev = nets[(dagger_name(n - 1), hint)]
+            net = ProposalNet(dev, seed=seed, uses_hint=hint)
             net.load_state_dict(prev.state_dict())
             cl2, ci2, cur2 = _starts(prob_t, kp_t, cfg_tr, seed + 5 * n)
             X2, Y2 = collect_learned(kp_t, prev, cl2, ci2, cur2, cfg_tr, seed + 5 * n + 1, log_cap)
             loss = net.fit(X2, Y2, epochs=epochs, batch=4096, lr=5e-4, seed=seed + n, log=log)
-            out["train"][f"{tgt}_moves"] = int(X2.shape[0])
+            out["train"][f"{tgt}{'_hint' if hint else ''}_moves"] = int(X2.shape[0])
             del X2, Y2
         else:
             Y = Yc if tgt == "chain" else Yl
-            net = ProposalNet(dev, seed=seed)
-            loss = net.fit(X, Y, epochs=epochs, batch=4096, lr=1e-3, seed=seed, log=log)
+            net = ProposalNet(dev, seed=seed, uses_hint=hint)
+            loss = net.fit(X if hint else without_hint(X), Y, epochs=epochs, batch=4096, lr=1e-3, seed=seed, log=log)
         e1.record()
         torch.cuda.synchronize(dev)
-        nets[tgt] = net
-        out["train"][tgt] = {"final_loss": loss, "train_ms": e0.elapsed_time(e1)}
+        nets[(tgt, hint)] = net
+        out["train"][tgt + ("_hint" if hint else "")] = {"final_loss": loss, "train_ms": e0.elapsed_time(e1)}
     del X, Yc, Yl, kp_t, prob_t
     # 2./3. evaluation on held-out ligands
     probs = {"f32": _problem_for(rec, eval_ligs, dev, "f32")}
@@ -362,9 +393,9 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
         ce, be = torch.zeros(cur.shape[0], device=dev), torch.full((cur.shape[0],), float("inf"), device=dev)
         st = {}
         if method in variants:
-            k, frac, tgt, tries = variants[method]
-            run_mc_segments(kp, nets[tgt], cl, ci, cur, ce, best, be, cfg, seed + 3, prop_k=k, prop_frac=frac,
-                            stats=st, prop_tries=tries)
+            k, frac, tgt, tries, hint = variants[method]
+            run_mc_segments(kp, nets[(tgt, hint)], cl, ci, cur, ce, best, be, cfg, seed + 3, prop_k=k,
+                            prop_frac=frac, stats=st, prop_tries=tries)
         else:
             kp.run_mc(cl, ci, cur, ce, best, be, True, steps, cfg["bfgs_iters"], cfg["mc_temperature"],
                       cfg["mc_amp_pos"], cfg["mc_amp_rot"], seed + 3, 0)
@@ -377,8 +408,8 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
 
     ref, ref_ms, ref_st = run("plain_f32", ref_steps)
     results = {}
-    out["learned_variants"] = {n: {"prop_k": k, "prop_frac": f, "target": t, "tries": r}
-                               for n, (k, f, t, r) in variants.items()}
+    out["learned_variants"] = {n: {"prop_k": k, "prop_frac": f, "target": t, "tries": r, "hint": h}
+                               for n, (k, f, t, r, h) in variants.items()}
     for m in ("plain_f32", *(("plain_f16",) if plain_f16 else ()), *variants):
         for S in (learned_budgets or budgets if m in variants else budgets):
             results[(m, S)] = run(m, S)
@@ -451,12 +482,13 @@ def run_mc_segments(kp, net, chain_lig, chain_id, cur, cur_e, best, best_e, cfg,
     pst = torch.zeros(4, dtype=torch.int64, device=kp.device)
     for sg in range(math.ceil(steps / prop_k)):
         k = min(prop_k, steps - sg * prop_k)
-        feat = kp.prop_features(chain_lig, cur)
+        hint = kp.prop_hint(chain_lig, best, best_e) if net.uses_hint and sg > 0 else None
+        feat = kp.prop_features(chain_lig, cur, cur_e, hint)
         out = net.forward(feat)
         moves = kp.prop_sample(chain_lig, chain_id, out, cur, k * prop_tries, seed ^ 0x5EEDBA5E, sg)
         kp.run_mc(chain_lig, chain_id, cur, cur_e, best, best_e, init_opt and sg == 0, k, cfg["bfgs_iters"],
                   cfg["mc_temperature"], cfg["mc_amp_pos"], cfg["mc_amp_rot"], seed, sg * prop_k, prop=moves,
-                  prop_stats=pst, prop_frac=prop_frac, log=log, prop_tries=prop_tries)
+                  prop_stats=pst, prop_frac=prop_frac, log=log, prop_tries=prop_tries, hint=hint)
     check_gemm("learned-proposal search")
     if stats is not None:
         p, pa, q, qa = pst.tolist()

@@ -121,7 +121,7 @@ typedef struct {
     const float* prop;
     int prop_k;
     unsigned long long* prop_stats; /* dev [4] or NULL: proposed, proposed+accepted, plain, plain+accepted */
-    /* training-data log (NULL = off): each accepted improving move appends features [288] (BF16) of the pre-move
+    /* training-data log (NULL = off): each accepted improving move appends features [320] (BF16) of the pre-move
      * state and that state [32] (t 3, q 4, torsions 20, torsion count at 27, chain index at 28) while
      * *log_n < cap; the training target (the move to the chain's final best state) is formed after the run */
     void* log_x;
@@ -135,6 +135,7 @@ typedef struct {
                                   evaluated once and BFGS runs from the lowest-energy one. prop then holds
                                   prop_k = steps x prop_tries targets per chain, the tries of a step consecutive.
                                   <= 1: one target per step */
+    const float* hint;         /* dev [L, 32] or NULL: ligand-best rows (adock_prop_hint) for the logged features */
 } adock_mc_args_t;
 
 /* ------------------------------------------------------------------------------------------------ misc */
@@ -275,13 +276,20 @@ int adock_rescore64(const adock_ligands_t* lig, const adock_work_t* work, const 
                     const float* state, double* e_total, double* e_intra, float* X, void* stream);
 
 /* ------------------------------------------------------------------------------------------------ proposal net */
-/* No reference counterpart: the learned MC proposal. Network 288 -> 256 (SiLU) -> 256 (SiLU) -> 64, BF16
+/* No reference counterpart: the learned MC proposal. Network 320 -> 256 (SiLU) -> 256 (SiLU) -> 64, BF16
  * weights, FP32 accumulation; output columns 0..25 = move means, 32..57 = log standard deviations. */
 
-/* Feature rows (BF16 [n, 288], dev) of n states (layout in csrc/search_impl.cuh prop_features). */
+/* Feature rows (BF16 [n, 320], dev) of n states (layout in csrc/search_impl.cuh prop_features). cur_e [n] (the
+ * states' energies) and hint [L, 32] (adock_prop_hint) may be NULL: the ligand-best columns are then 0. */
 int adock_prop_features(const adock_ligands_t* lig, const adock_work_t* work, const adock_grids_t* grids,
-                        const adock_sf_t* sf, const int* chain_lig, int n, const float* state, void* feat,
-                        void* stream);
+                        const adock_sf_t* sf, const int* chain_lig, int n, const float* state, const float* cur_e,
+                        const float* hint, void* feat, void* stream);
+/* Ligand-best rows hint [L, 32] (dev): for each ligand, the best state (t 3, q 4, torsions 0..19) of its chain with
+ * the lowest finite best_e (ties: the lowest chain index), that energy at 27 and 1 at 28; all 0 for a ligand
+ * without such a chain. best [n, SD] and best_e [n] are the chains' best states and energies; keys is device
+ * scratch of L x 8 bytes. */
+int adock_prop_hint(int L, int n, const int* chain_lig, const float* best, int SD, const float* best_e, void* keys,
+                    float* hint, void* stream);
 /* Proposed target states [n, k, 32] (dev; t 3, q 4, torsions 20, rest 0) drawn from the network output [n, 64]
  * around the states state [n, SD] the network read: move = mean + max(exp(log_sd), floor) * z, z standard normal
  * from a counter-based stream of (seed, chain_id, segment, slot), applied to the state (translation added,

@@ -20,7 +20,7 @@ def _dsilu(a):
 
 
 def loss_and_grads(W, b, X, Y):
-    """W: 3 arrays [K, N]; b: 3 arrays [N]; X [B, 288]; Y [B, 32]. Returns (loss, [dW1, dW2, dW3, db1, db2, db3])."""
+    """W: 3 arrays [K, N]; b: 3 arrays [N]; X [B, 320]; Y [B, 32]. Returns (loss, [dW1, dW2, dW3, db1, db2, db3])."""
     W = [np.asarray(w, np.float64) for w in W]
     b = [np.asarray(v, np.float64) for v in b]
     X = np.asarray(X, np.float64)

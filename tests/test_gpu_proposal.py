@@ -83,7 +83,8 @@ def test_network_gradients_match_float64_oracle(dev):
     net.Wb = [w.to(torch.bfloat16).contiguous() for w in net.W]
     g = torch.Generator(device=dev).manual_seed(1)
     B = 512
-    X = torch.randn(B, 288, device=dev, generator=g).to(torch.bfloat16)
+    from adock_b200.proposal import IN
+    X = torch.randn(B, IN, device=dev, generator=g).to(torch.bfloat16)
     Y = torch.randn(B, 32, device=dev, generator=g) * 0.5
     Y[:, 26] = torch.randint(0, 21, (B,), device=dev, generator=g).float()
     Y[:, 27:] = 0
@@ -130,7 +131,7 @@ def test_features_log_training_and_proposal_mc(dev):
     ci = torch.arange(M, dtype=torch.int32, device=dev)
     # feature rows: finite, torsion sin/cos zero beyond each ligand's count, descriptors as documented
     F = kp.prop_features(cl, st).float().cpu().numpy()
-    assert F.shape == (M, 288) and np.isfinite(F).all()
+    assert F.shape == (M, 320) and np.isfinite(F).all()
     for i in range(M):
         p = prob.lb.preps[int(cl[i])]
         assert abs(F[i, 263] - p.n / 64) < 1e-2 and abs(F[i, 264] - p.n_tors / 20) < 1e-2
@@ -168,6 +169,90 @@ def test_features_log_training_and_proposal_mc(dev):
     assert X2.shape[0] > M and X2.shape[0] == Y2.shape[0]
     Y2n = Y2.cpu().numpy()
     assert np.isfinite(Y2n).all() and np.all(np.abs(Y2n[:, 6:26]) <= np.pi + 1e-4)
+
+
+def _wrap(d):
+    return d - 2 * np.pi * np.floor((d + np.pi) / (2 * np.pi))
+
+
+def test_ligand_best_hint(dev):
+    """adock_prop_hint picks, per ligand, the chain with the lowest finite best energy (ties: the lowest chain
+    index; non-finite energies never win) and copies its state; the feature row's hint columns equal a float64
+    restatement (translation / rotation-vector / torsion differences, energy terms); segmenting the plain search
+    for the hint leaves its moves unchanged."""
+    from adock_b200 import params
+    from adock_b200.kernel import B200KernelProblem
+    from adock_b200.proposal import HINT_COLS, collect, without_hint
+    prob = _problem(dev)
+    kp = B200KernelProblem(prob)
+    L = prob.lb.L
+    cl, st = random_states(prob, 12, seed=4, sigma=1.5)
+    M = len(cl)
+    cln = np.asarray(cl)
+    rng = np.random.default_rng(3)
+    be = rng.normal(-5, 2, M).astype(np.float32)
+    be[rng.random(M) < 0.1] = np.inf
+    be[rng.random(M) < 0.05] = np.nan
+    l0 = np.where(cln == 0)[0]
+    be[l0] = np.inf                      # ligand 0: no finite energy -> no hint
+    l1 = np.where(cln == 1)[0]
+    be[l1[1]] = be[l1[3]] = -50.0        # tie: the lower chain index wins
+    clg, stg = torch.as_tensor(cl, device=dev), torch.as_tensor(st, device=dev)
+    hint = kp.prop_hint(clg, stg, torch.as_tensor(be, device=dev)).cpu().numpy()
+    for l in range(L):
+        ch = np.where((cln == l) & np.isfinite(be))[0]
+        if len(ch) == 0:
+            assert np.all(hint[l] == 0), l
+            continue
+        w = ch[np.argmin(be[ch])]
+        assert l != 1 or w == l1[1]
+        K = min(20, st.shape[1] - 7)
+        np.testing.assert_array_equal(hint[l, :7 + K], st[w, :7 + K])
+        assert hint[l, 27] == be[w] and hint[l, 28] == 1.0
+    # hint columns of the feature rows
+    ce = rng.normal(-3, 2, M).astype(np.float32)
+    F = kp.prop_features(clg, stg, torch.as_tensor(ce, device=dev), torch.as_tensor(hint, device=dev))
+    F = F.float().cpu().numpy()
+    F0 = kp.prop_features(clg, stg).float().cpu().numpy()
+    other = [c for c in range(320) if c not in HINT_COLS]
+    np.testing.assert_array_equal(F[:, other], F0[:, other])
+    assert np.all(F0[:, HINT_COLS] == 0)
+    slog = lambda v: np.sign(v) * np.log1p(np.abs(v))
+    for i in range(M):
+        h = hint[cln[i]].astype(np.float64)
+        s = st[i].astype(np.float64)
+        if h[28] == 0:
+            assert np.all(F[i, HINT_COLS] == 0)
+            continue
+        qa = s[3:7] / np.linalg.norm(s[3:7])
+        qb = h[3:7] / np.linalg.norm(h[3:7])
+        aw, av = qa[0], -qa[1:]
+        r = np.concatenate([[qb[0] * aw - qb[1:] @ av], qb[0] * av + aw * qb[1:] + np.cross(qb[1:], av)])
+        r = r if r[0] >= 0 else -r
+        sn = np.linalg.norm(r[1:])
+        rv = r[1:] * 2 * np.arctan2(sn, r[0]) / max(sn, 1e-300) / np.pi
+        nt = prob.lb.preps[cln[i]].n_tors
+        want = np.concatenate([(h[:3] - s[:3]) / 10, rv, [slog(ce[i] - h[27]), slog(ce[i]), 1.0]])
+        tw = np.zeros(20)
+        tw[:nt] = _wrap(h[7:7 + nt] - s[7:7 + nt]) / np.pi
+        got = F[i, HINT_COLS]
+        # BF16 rows: 2^-8 relative; wrapped torsion differences near +-pi may land on either end
+        assert np.all(np.abs(got[:9] - want) <= 1e-2 * np.maximum(np.abs(want), 0.1)), (i, got[:9], want)
+        dt = np.abs(got[9:] - tw)
+        assert np.all((dt <= 1e-2) | (np.abs(dt - 2) <= 1e-2)), (i, got[9:], tw)
+    np.testing.assert_array_equal(without_hint(torch.as_tensor(F)).numpy()[:, HINT_COLS], 0)
+    # the segmented plain search (hint in the logged features) makes the same moves as one launch
+    cfg = params.workload_preset(32, 12)
+    res = []
+    for hs in (0, 4):
+        cur, best = stg.clone(), stg.clone()
+        c_e, b_e = torch.zeros(M, device=dev), torch.full((M,), float("inf"), device=dev)
+        X, Y = collect(kp, clg, torch.arange(M, dtype=torch.int32, device=dev), cur, c_e, best, b_e, cfg, seed=5,
+                       cap=100000, hint_segment=hs)
+        res.append((best.cpu(), b_e.cpu(), X))
+    torch.testing.assert_close(res[0][1], res[1][1], rtol=0, atol=0)
+    torch.testing.assert_close(res[0][0], res[1][0], rtol=0, atol=0)
+    assert (res[1][2][:, HINT_COLS[-20:]] != 0).any() and (res[0][2][:, HINT_COLS] == 0).all()
 
 
 def test_trained_proposal_beats_plain_mc_at_equal_budget(dev):
