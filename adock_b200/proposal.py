@@ -303,6 +303,74 @@ def _best_per_ligand(best_e, L, M):
     return best_e.view(L, M).min(1).values
 
 
+def parse_learned(learned):
+    """Learned variants (name, segment steps, learned fraction[, training "chain" | "ligand" | "dagger" |
+    "daggerN"[, tries[, hint]]]) -> {name: (prop_k, prop_frac, target, tries, hint)}: the chain's or the ligand's
+    best pose as target, or the chain network fine-tuned N times on its own search's moves; tries candidate
+    targets per learned step; hint: the network reads the ligand-best hint."""
+    return {v[0]: (v[1], v[2], v[3] if len(v) > 3 else "chain", int(v[4]) if len(v) > 4 else 1,
+                   bool(v[5]) if len(v) > 5 else False) for v in learned}
+
+
+def _rounds(t):   # "dagger" = 1 self-training round on top of "chain", "dagger2" = 2, ...
+    return int(t[6:] or 1) if t.startswith("dagger") else 0
+
+
+def _dagger_name(n):
+    return "chain" if n == 0 else ("dagger" if n == 1 else f"dagger{n}")
+
+
+def train_variants(rec, train_ligs, variants, device="cuda", chains=32, train_steps=500, log_cap=2_000_000,
+                   epochs=3, seed=0, log=None):
+    """Train the networks the learned variants need (values of ``parse_learned``) on fresh ligands: the plain FP32
+    search (Stage-A starts, ``train_steps`` MC steps) logs its improving moves, a network is fitted to them, and
+    each self-training round lets the previous round's network drive the search on the training ligands and
+    fine-tunes a copy on that search's moves. Returns ({(target, hint): net}, training record)."""
+    from . import params
+    dev = torch.device(device)
+    variants = list(variants)
+    cfg_tr = params.workload_preset(chains, train_steps)
+    prob_t, kp_t = _problem_for(rec, train_ligs, dev)
+    cl, ci, cur = _starts(prob_t, kp_t, cfg_tr, seed)
+    N = cur.shape[0]
+    best = cur.clone()
+    ce, be = torch.zeros(N, device=dev), torch.full((N,), float("inf"), device=dev)
+    torch.cuda.synchronize(dev)
+    any_hint = any(h for (_, _, _, _, h) in variants)
+    X, Yc, Yl = collect(kp_t, cl, ci, cur, ce, best, be, cfg_tr, seed=seed + 1, cap=log_cap, target="both",
+                        hint_segment=32 if any_hint else 0)
+    nets = {}
+    rec_out = {"moves": int(X.shape[0]), "epochs": epochs}
+    targets = {(t, h) for (_, _, t, _, h) in variants}
+    for (t, h) in list(targets):
+        for n in range(_rounds(t)):
+            targets.add((_dagger_name(n), h))
+    for (tgt, hint) in sorted(targets, key=lambda th: (th[1], th[0] == "ligand", _rounds(th[0]))):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        n = _rounds(tgt)
+        if n > 0:
+            # self-training round n: the previous round's network drives the search on the training ligands with
+            # the log on; a copy of it is fine-tuned on those moves (targets: that search's own final minima)
+            prev = nets[(_dagger_name(n - 1), hint)]
+            net = ProposalNet(dev, seed=seed, uses_hint=hint)
+            net.load_state_dict(prev.state_dict())
+            cl2, ci2, cur2 = _starts(prob_t, kp_t, cfg_tr, seed + 5 * n)
+            X2, Y2 = collect_learned(kp_t, prev, cl2, ci2, cur2, cfg_tr, seed + 5 * n + 1, log_cap)
+            loss = net.fit(X2, Y2, epochs=epochs, batch=4096, lr=5e-4, seed=seed + n, log=log)
+            rec_out[f"{tgt}{'_hint' if hint else ''}_moves"] = int(X2.shape[0])
+            del X2, Y2
+        else:
+            Y = Yc if tgt == "chain" else Yl
+            net = ProposalNet(dev, seed=seed, uses_hint=hint)
+            loss = net.fit(X if hint else without_hint(X), Y, epochs=epochs, batch=4096, lr=1e-3, seed=seed, log=log)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        nets[(tgt, hint)] = net
+        rec_out[tgt + ("_hint" if hint else "")] = {"final_loss": loss, "train_ms": e0.elapsed_time(e1)}
+    return nets, rec_out
+
+
 def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(125, 250, 500, 1000, 2000),
                ref_steps=8000, train_steps=500, log_cap=2_000_000, epochs=3, learned=(("learned_f16", 32, 0.3),),
                seed=0, log=None, learned_budgets=None, plain_f16=True):
@@ -319,63 +387,14 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
        and per second. ``learned_budgets`` limits the learned variants' budgets; ``plain_f16=False`` skips the plain
        FP16 rows.
     """
-    dev = torch.device(device)
     from . import params
-    cfg_tr = params.workload_preset(chains, train_steps)
+    dev = torch.device(device)
     out = {"chains": chains, "budgets": list(budgets), "ref_steps": ref_steps, "train_ligands": len(train_ligs),
            "eval_ligands": len(eval_ligs)}
+    variants = parse_learned(learned)
     # 1. data + training
-    prob_t, kp_t = _problem_for(rec, train_ligs, dev)
-    cl, ci, cur = _starts(prob_t, kp_t, cfg_tr, seed)
-    N = cur.shape[0]
-    best = cur.clone()
-    ce, be = torch.zeros(N, device=dev), torch.full((N,), float("inf"), device=dev)
-    torch.cuda.synchronize(dev)
-    # learned variants: (name, segment steps, learned fraction[, training "chain" | "ligand" | "dagger" |
-    # "daggerN"[, tries[, hint]]]): the chain's or the ligand's best pose as target, or the chain network
-    # fine-tuned N times on its own search's moves; tries candidate targets per learned step; hint: the network
-    # reads the ligand-best hint
-    variants = {v[0]: (v[1], v[2], v[3] if len(v) > 3 else "chain", int(v[4]) if len(v) > 4 else 1,
-                       bool(v[5]) if len(v) > 5 else False) for v in learned}
-    any_hint = any(h for (_, _, _, _, h) in variants.values())
-    X, Yc, Yl = collect(kp_t, cl, ci, cur, ce, best, be, cfg_tr, seed=seed + 1, cap=log_cap, target="both",
-                        hint_segment=32 if any_hint else 0)
-    nets = {}
-    out["train"] = {"moves": int(X.shape[0]), "epochs": epochs}
-    def rounds(t):   # "dagger" = 1 self-training round on top of "chain", "dagger2" = 2, ...
-        return int(t[6:] or 1) if t.startswith("dagger") else 0
-
-    def dagger_name(n):
-        return "chain" if n == 0 else ("dagger" if n == 1 else f"dagger{n}")
-
-    targets = {(t, h) for (_, _, t, _, h) in variants.values()}
-    for (t, h) in list(targets):
-        for n in range(rounds(t)):
-            targets.add((dagger_name(n), h))
-    for (tgt, hint) in sorted(targets, key=lambda th: (th[1], th[0] == "ligand", rounds(th[0]))):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        n = rounds(tgt)
-        if n > 0:
-            # self-training round n: the previous round's network drives the search on the training ligands with
-            # the log on; a copy of it is fine-tuned on those moves (targets: that search's own final minima)
-            prev = nets[(dagger_name(n - 1), hint)]
-            net = ProposalNet(dev, seed=seed, uses_hint=hint)
-            net.load_state_dict(prev.state_dict())
-            cl2, ci2, cur2 = _starts(prob_t, kp_t, cfg_tr, seed + 5 * n)
-            X2, Y2 = collect_learned(kp_t, prev, cl2, ci2, cur2, cfg_tr, seed + 5 * n + 1, log_cap)
-            loss = net.fit(X2, Y2, epochs=epochs, batch=4096, lr=5e-4, seed=seed + n, log=log)
-            out["train"][f"{tgt}{'_hint' if hint else ''}_moves"] = int(X2.shape[0])
-            del X2, Y2
-        else:
-            Y = Yc if tgt == "chain" else Yl
-            net = ProposalNet(dev, seed=seed, uses_hint=hint)
-            loss = net.fit(X if hint else without_hint(X), Y, epochs=epochs, batch=4096, lr=1e-3, seed=seed, log=log)
-        e1.record()
-        torch.cuda.synchronize(dev)
-        nets[(tgt, hint)] = net
-        out["train"][tgt + ("_hint" if hint else "")] = {"final_loss": loss, "train_ms": e0.elapsed_time(e1)}
-    del X, Yc, Yl, kp_t, prob_t
+    nets, out["train"] = train_variants(rec, train_ligs, variants.values(), dev, chains=chains,
+                                        train_steps=train_steps, log_cap=log_cap, epochs=epochs, seed=seed, log=log)
     # 2./3. evaluation on held-out ligands
     probs = {"f32": _problem_for(rec, eval_ligs, dev, "f32")}
     probs["f16"] = (probs["f32"][0], type(probs["f32"][1])(probs["f32"][0], grid_dtype="f16"))
@@ -451,6 +470,86 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
         if c.get(m) and c.get("plain_f32"):
             out[f"speedup_interp_at_gap_0.1_{m}"] = c[m]["ligands_per_s"] / c["plain_f32"]["ligands_per_s"]
     return out
+
+
+def full_screen(rec, train_ligs, screen_ligs, variant, device="cuda", chains=32, learned_steps=500,
+                plain_steps=3000, ref_steps=8000, n_sub=1024, train_steps=500, log_cap=4_000_000, epochs=3, seed=0,
+                log=None):
+    """The full-form screening run: all of ``screen_ligs`` docked in one batch by the learned FP16 search
+    (``variant`` as in ``parse_learned``) at ``learned_steps`` and by the plain FP32 search at ``plain_steps``, each
+    timed with CUDA events from Stage A to the end of the MC phase, with the launch variant the autotuner picks for
+    the batch (tuned before the timed runs). The median best-energy gap of both runs is measured on the first
+    ``n_sub`` ligands against a ``ref_steps`` plain FP32 run of that subset (floor: the lowest energy any of the
+    three runs found for the ligand)."""
+    from . import params
+    dev = torch.device(device)
+    v = parse_learned([variant])
+    name, (k, frac, tgt, tries, hint) = next(iter(v.items()))
+    t_train = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t_train[0].record()
+    nets, train_rec = train_variants(rec, train_ligs, v.values(), dev, chains=chains, train_steps=train_steps,
+                                     log_cap=log_cap, epochs=epochs, seed=seed, log=log)
+    t_train[1].record()
+    net = nets[(tgt, hint)]
+    del nets
+    L = len(screen_ligs)
+    n_sub = min(n_sub, L)
+    prob, kp32 = _problem_for(rec, screen_ligs, dev, "f32")
+    kp16 = type(kp32)(prob, grid_dtype="f16")
+
+    def run(kp, steps, learned):
+        cfg = params.workload_preset(chains, steps)
+        cfg["autotune"] = False
+        ev0 = int(kp.evals[0])
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record()
+        cl, ci, cur = _starts(prob, kp, cfg, seed + 2)
+        ev[1].record()
+        best = cur.clone()
+        ce, be = torch.zeros(cur.shape[0], device=dev), torch.full((cur.shape[0],), float("inf"), device=dev)
+        st = {}
+        if learned:
+            run_mc_segments(kp, net, cl, ci, cur, ce, best, be, cfg, seed + 3, prop_k=k, prop_frac=frac, stats=st,
+                            prop_tries=tries)
+        else:
+            kp.run_mc(cl, ci, cur, ce, best, be, True, steps, cfg["bfgs_iters"], cfg["mc_temperature"],
+                      cfg["mc_amp_pos"], cfg["mc_amp_rot"], seed + 3, 0)
+        ev[2].record()
+        torch.cuda.synchronize(dev)
+        ms = ev[0].elapsed_time(ev[2])
+        n_ev = int(kp.evals[0]) - ev0
+        row = {"steps": steps, "ms": ms, "stage_a_ms": ev[0].elapsed_time(ev[1]), "ligands_per_s": L / (ms / 1e3),
+               "evals_per_s": n_ev / (ev[1].elapsed_time(ev[2]) / 1e3), "evals_per_step": n_ev / (cur.shape[0] * steps),
+               "mc_variant": int(getattr(kp, "mc_variant", 0)), **st}
+        return _best_per_ligand(be, L, chains), row
+
+    # the launch variant for this batch (autotuner samples on the Stage-A starts, untimed)
+    for kp in (kp32, kp16):
+        cl, _, cur = _starts(prob, kp, params.workload_preset(chains, 1), seed + 2)
+        kp.tune(cl, cur)
+    e_l, row_l = run(kp16, learned_steps, True)
+    e_p, row_p = run(kp32, plain_steps, False)
+    # gap floor on the subset: a long plain FP32 run of its ligands
+    prob_s, kp_s = _problem_for(rec, screen_ligs[:n_sub], dev, "f32")
+    cfg_r = params.workload_preset(chains, ref_steps)
+    cfg_r["autotune"] = False
+    cl, ci, cur = _starts(prob_s, kp_s, cfg_r, seed + 4)
+    best = cur.clone()
+    ce, be = torch.zeros(cur.shape[0], device=dev), torch.full((cur.shape[0],), float("inf"), device=dev)
+    kp_s.run_mc(cl, ci, cur, ce, best, be, True, ref_steps, cfg_r["bfgs_iters"], cfg_r["mc_temperature"],
+                cfg_r["mc_amp_pos"], cfg_r["mc_amp_rot"], seed + 5, 0)
+    e_ref = _best_per_ligand(be, n_sub, chains)
+    floor = torch.minimum(torch.minimum(e_ref, e_l[:n_sub]), e_p[:n_sub])
+    for e, row in ((e_l, row_l), (e_p, row_p)):
+        gap = (e[:n_sub] - floor).cpu()
+        row.update(median_gap=float(gap.median()), mean_gap=float(gap.mean()))
+    torch.cuda.synchronize(dev)
+    return {"ligands": L, "chains": chains, "gap_subset": n_sub, "ref_steps": ref_steps, "train_ligands": len(train_ligs),
+            "train": train_rec, "train_ms": t_train[0].elapsed_time(t_train[1]), "learned_variant": {
+                "name": name, "prop_k": k, "prop_frac": frac, "target": tgt, "tries": tries, "hint": hint},
+            "learned_f16": row_l, "plain_f32": row_p,
+            "speedup_ligands_per_s": row_l["ligands_per_s"] / row_p["ligands_per_s"],
+            "both_within_gap_0.1": row_l["median_gap"] <= 0.1 and row_p["median_gap"] <= 0.1}
 
 
 def interp_to_gap(rows, gap):

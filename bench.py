@@ -69,6 +69,16 @@ def _args():
     ap.add_argument("--screen-variants", default="learned_dagger2:32:0.3:dagger2:4",
                     help="learned variants of the screening comparison (as --ab-variants; dagger, dagger2, ...: "
                          "that many self-training rounds)")
+    ap.add_argument("--screen-full", action="store_true",
+                    help="the full-form screening run in place of the bench line: --screen-full-ligands ligands on "
+                         "the 8,000-atom receptor docked in one batch by the learned FP16 search and by the plain FP32 "
+                         "search, gaps on a subset, the reference's CPU search on a sample")
+    ap.add_argument("--screen-full-ligands", type=int, default=16384)
+    ap.add_argument("--screen-full-learned-steps", type=int, default=500)
+    ap.add_argument("--screen-full-plain-steps", type=int, default=3000)
+    ap.add_argument("--screen-full-subset", type=int, default=1024, help="ligands whose gap is measured")
+    ap.add_argument("--screen-full-cpu", type=int, default=16,
+                    help="ligands of the first 256 timed with the reference's CPU search (0: none)")
     return ap.parse_args()
 
 
@@ -503,6 +513,56 @@ def _cpu_baseline(ligs, rec, cfg):
                       f"{cfg['mc_steps']} steps, one full stock search, {dt:.1f} s"}
 
 
+def run_screen_full(args):
+    """The full-form screening workload (configs of the screening run: FP16 maps, learned proposal, 32 chains per
+    ligand, ligands with 8-80 heavy atoms and 0-20 torsions against the 8,000-atom receptor) as one batch, against
+    the plain FP32 search of the same batch; the reference's CPU search on a quantile sample of the first 256
+    ligands at the plain budget."""
+    import numpy as np
+    import torch
+    from adock_b200 import params, synth
+    from adock_b200.proposal import full_screen
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    rec2 = synth.config_receptor(2)
+    train = synth.ligand_set(args.screen_train, (8, 80), (0, 20), seed0=300_000)
+    ligs = synth.ligand_set(args.screen_full_ligands, (8, 80), (0, 20), seed0=700_000)
+    variant = next(v for v in args.screen_variants.split(",") if v)
+    f = variant.split(":")
+    variant = (f[0], int(f[1]), float(f[2])) + ((f[3],) if len(f) > 3 else ()) + \
+        ((int(f[4]),) if len(f) > 4 else ()) + ((f[5] in ("1", "hint"),) if len(f) > 5 else ())
+    clocks = ClockSampler(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0])
+    t0 = time.perf_counter()
+    res = full_screen(rec2, train, ligs, variant, device=dev, learned_steps=args.screen_full_learned_steps,
+                      plain_steps=args.screen_full_plain_steps, n_sub=args.screen_full_subset,
+                      log_cap=args.screen_log_cap)
+    res["wall_s"] = time.perf_counter() - t0
+    res["clocks"] = clocks.stop()
+    out = {"metric": "ligands docked/s at equal median best-energy gap: learned FP16 vs plain FP32 search", "unit": UNIT,
+           "workload": f"full-form screening: {len(ligs)} ligands (8-80 heavy atoms, 0-20 torsions) x 32 chains vs "
+                       "the 8,000-atom receptor (30 A box, 81^3 x 8 maps); learned FP16 vs plain FP32",
+           "data": "synthetic (seeded)", "screen_full": res}
+    if args.screen_full_cpu > 0:
+        A = _stock_reference()
+        if A is None:
+            out["cpu_baseline"] = {"value": None, "sample": "unavailable: the reference package is not installed"}
+        else:
+            torch.set_num_threads(A.threads)
+            sub = ligs[:256]
+            order = sorted(range(len(sub)), key=lambda i: (sub[i].n, i))
+            n = args.screen_full_cpu
+            sample = [sub[order[int(len(order) * (j + 0.5) / n)]] for j in range(n)]
+            cfg = params.workload_preset(32, args.screen_full_plain_steps)
+            prob = _reference_problem(A, rec2, sample)
+            _reference_search(A, prob, dict(cfg, mc_steps=20, mc_segment=20))    # compile + page in (untimed)
+            dt, _ = _reference_search(A, prob, cfg)
+            out["cpu_baseline"] = {"value": len(sample) / dt, "unit": UNIT, "cores": A.threads, "kind": "reference",
+                                   "sample": f"{len(sample)} ligands at the quantiles of the heavy-atom count of the "
+                                             f"first 256 x 32 chains x {cfg['mc_steps']} steps (the plain budget), "
+                                             f"one full stock search, {dt:.1f} s"}
+    return out
+
+
 def main():
     args = _args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -520,6 +580,8 @@ def main():
             dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=180))
     if args.impl == "reference":
         out = run_reference(args, rank, world)
+    elif args.screen_full:
+        out = run_screen_full(args) if rank == 0 else None
     else:
         out = run_ours(args, rank, world, local_rank)
     if rank == 0 and out is not None:
