@@ -275,7 +275,9 @@ __device__ __forceinline__ float pair_slot(int2 pr, const float* X, float* F, co
 // translation; trilinear grid (or exact pairwise) inter energy with the quadratic out-of-box penalty; intra
 // pairs. Gradient: dE/dt = sum F, torque = sum (X - t) x F, dE/dtheta_k = u_k . sum_{a moved by k} (X_a - p_k) x F_a,
 // evaluated as u_k . (sum X' x F - p'_k x sum F) over the subtree of k (X' = X - t).
-template <int APL, typename GT>
+// EX selects the inter energy at compile time: exact pairwise over receptor atoms (or the chain's neighbour list),
+// else the trilinear grid, so the grid-mode kernels carry no receptor loop.
+template <int APL, typename GT, bool EX>
 __device__ __forceinline__ float eval_eg(float* ws, const WSLayout& L, const float* s, float* g, const Chain<APL>& c,
                          const SearchParams& P, const TypeTables& tt, int lane) {
     constexpr int AM = 32 * APL;
@@ -331,7 +333,7 @@ __device__ __forceinline__ float eval_eg(float* ws, const WSLayout& L, const flo
             X[AM + a] = X1;
             X[2 * AM + a] = X2;
             float ea, gg[3];
-            if (c.exact) {
+            if constexpr (EX) {
                 ea = 0.f;
                 gg[0] = gg[1] = gg[2] = 0.f;
                 const int ta = c.typ[i] & 63;
@@ -503,7 +505,7 @@ __device__ __forceinline__ void neg_hv(const float* H, const float* v, float* ou
 // Not inlined: the MC kernel calls it from two sites (start optimisation and every step); one copy, with one
 // inlined eval_eg, keeps the kernel small enough for the instruction cache (instruction-fetch stalls were the
 // largest stall reason with four inlined copies of eval_eg).
-template <int APL, typename GT>
+template <int APL, typename GT, bool EX>
 __device__ ADOCK_BFGS_ATTR float bfgs(float* ws, const WSLayout& L, float* x, int iters, const Chain<APL>& c_in,
                                    const SearchParams& P, const TypeTables& tt, int lane, unsigned& n_eval) {
     const Chain<APL> c = c_in;   // registers for the whole optimisation
@@ -523,7 +525,7 @@ __device__ ADOCK_BFGS_ATTR float bfgs(float* ws, const WSLayout& L, float* x, in
     int step = 0, trial = 0;
     bool first = true;
     while (true) {
-        const float f = eval_eg<APL, GT>(ws, L, first ? x : xn, first ? g : gn, c, P, tt, lane);
+        const float f = eval_eg<APL, GT, EX>(ws, L, first ? x : xn, first ? g : gn, c, P, tt, lane);
         ++n_eval;
         if (first) {
             first = false;
@@ -720,7 +722,7 @@ static __device__ ADOCK_COLD_ATTR void log_state(const float* s, int nt, int ch,
     for (int t = 29; t < 32; ++t) y[t] = 0.f;
 }
 
-template <int APL, typename GT, int MINB>
+template <int APL, typename GT, int MINB, bool EX>
 __global__ void __launch_bounds__(128, MINB) mc_kernel(const __grid_constant__ SearchParams P,
                                                        const __grid_constant__ McParams M,
                                                        const __grid_constant__ TypeTables ttg) {
@@ -760,7 +762,7 @@ __global__ void __launch_bounds__(128, MINB) mc_kernel(const __grid_constant__ S
         }
         __syncwarp();
         float ec, eb = M.best_e[ch];
-        if (M.init_opt) ec = bfgs<APL, GT>(ws, L, cur, iters, c, P, tt, lane, n_eval);
+        if (M.init_opt) ec = bfgs<APL, GT, EX>(ws, L, cur, iters, c, P, tt, lane, n_eval);
         else ec = M.cur_e[ch];
         if (ec < eb) {
             eb = ec;
@@ -791,7 +793,7 @@ __global__ void __launch_bounds__(128, MINB) mc_kernel(const __grid_constant__ S
                         for (int k = lane; k < c.nt && k < 20; k += 32) x[7 + k] = mv[7 + k];
                         __syncwarp();
                         if (!target_finite(x, c.nt, lane)) continue;
-                        const float et = bfgs<APL, GT>(ws, L, x, 0, c, P, tt, lane, n_eval);   // one evaluation
+                        const float et = bfgs<APL, GT, EX>(ws, L, x, 0, c, P, tt, lane, n_eval);   // one evaluation
                         if (et < e_min) { e_min = et; pick = tr; }
                     }
                     wcopy(x, cur, S, lane);
@@ -819,7 +821,7 @@ __global__ void __launch_bounds__(128, MINB) mc_kernel(const __grid_constant__ S
                 }
             }
             __syncwarp();
-            const float en = skip ? 3.4e38f : bfgs<APL, GT>(ws, L, x, iters, c, P, tt, lane, n_eval);
+            const float en = skip ? 3.4e38f : bfgs<APL, GT, EX>(ws, L, x, iters, c, P, tt, lane, n_eval);
             const bool accept =
                 isfinite(en) && ((en < ec) || (uniform01(M.seed, cid, sg, 2) < __expf((ec - en) / M.temp)));
             if (use_prop) { ++n_prop; n_prop_acc += accept; } else { ++n_plain; n_plain_acc += accept; }
@@ -865,7 +867,7 @@ __global__ void __launch_bounds__(128, MINB) mc_kernel(const __grid_constant__ S
     }
 }
 
-template <int APL, typename GT>
+template <int APL, typename GT, bool EX>
 __global__ void __launch_bounds__(128) eg_kernel(const __grid_constant__ SearchParams P, const int* chain_lig, int n,
                                                  const float* state, float* e_out, float* g_out, int exact,
                                                  const __grid_constant__ TypeTables ttg) {
@@ -885,7 +887,7 @@ __global__ void __launch_bounds__(128) eg_kernel(const __grid_constant__ SearchP
         float* g = ws + L.g;
         for (int i = lane; i < SDM; i += 32) x[i] = state[(long long)ch * SDM + i];
         __syncwarp();
-        const float e = eval_eg<APL, GT>(ws, L, x, g, c, P, tt, lane);
+        const float e = eval_eg<APL, GT, EX>(ws, L, x, g, c, P, tt, lane);
         for (int i = lane; i < 6 + c.nt; i += 32) g_out[(long long)ch * DMM + i] = g[i];
         if (lane == 0) e_out[ch] = e;
         __syncwarp();
@@ -1120,7 +1122,7 @@ static int launch_mc_v(const SearchParams& P, const McParams& M, const TypeTable
     const int wpb = 4;
     const WSLayout L(P.AM, P.KM);
     const size_t smem = (size_t)wpb * L.total * sizeof(float);
-    auto kern = mc_kernel<APL, GT, MINB>;
+    auto kern = M.exact ? mc_kernel<APL, GT, MINB, true> : mc_kernel<APL, GT, MINB, false>;
     ADOCK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     ADOCK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * wpb, smem));
@@ -1160,7 +1162,7 @@ static int launch_eg_t(const SearchParams& P, const int* cl, int n, const float*
     const int wpb = 4;
     const WSLayout L(P.AM, P.KM);
     const size_t smem = (size_t)wpb * L.total * sizeof(float);
-    auto kern = eg_kernel<APL, GT>;
+    auto kern = exact ? eg_kernel<APL, GT, true> : eg_kernel<APL, GT, false>;
     ADOCK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     long long blocks = (n + wpb - 1) / wpb;
     const long long cap = (long long)sm_count() * 16;

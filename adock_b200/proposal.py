@@ -472,15 +472,16 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
     return out
 
 
-def full_screen(rec, train_ligs, screen_ligs, variant, device="cuda", chains=32, learned_steps=500,
+def full_screen(rec, train_ligs, screen_ligs, variant, device="cuda", chains=32, learned_steps=(400, 600),
                 plain_steps=3000, ref_steps=8000, n_sub=1024, train_steps=500, log_cap=4_000_000, epochs=3, seed=0,
                 log=None):
     """The full-form screening run: all of ``screen_ligs`` docked in one batch by the learned FP16 search
-    (``variant`` as in ``parse_learned``) at ``learned_steps`` and by the plain FP32 search at ``plain_steps``, each
-    timed with CUDA events from Stage A to the end of the MC phase, with the launch variant the autotuner picks for
-    the batch (tuned before the timed runs). The median best-energy gap of both runs is measured on the first
-    ``n_sub`` ligands against a ``ref_steps`` plain FP32 run of that subset (floor: the lowest energy any of the
-    three runs found for the ligand)."""
+    (``variant`` as in ``parse_learned``) at each budget of ``learned_steps`` and by the plain FP32 search at
+    ``plain_steps``, each timed with CUDA events from Stage A to the end of the MC phase, with the launch variant
+    the autotuner picks for the batch (tuned before the timed runs). The median best-energy gap of every run is
+    measured on the first ``n_sub`` ligands against a ``ref_steps`` plain FP32 run of that subset (floor: the lowest
+    energy any run found for the ligand). At equal gap: the learned budget that reaches the plain run's median gap
+    (and the 0.1 kcal/mol bar), interpolated between the learned budgets as in ``interp_to_gap``."""
     from . import params
     dev = torch.device(device)
     v = parse_learned([variant])
@@ -527,7 +528,7 @@ def full_screen(rec, train_ligs, screen_ligs, variant, device="cuda", chains=32,
     for kp in (kp32, kp16):
         cl, _, cur = _starts(prob, kp, params.workload_preset(chains, 1), seed + 2)
         kp.tune(cl, cur)
-    e_l, row_l = run(kp16, learned_steps, True)
+    learned = [run(kp16, S, True) for S in sorted(learned_steps)]
     e_p, row_p = run(kp32, plain_steps, False)
     # gap floor on the subset: a long plain FP32 run of its ligands
     prob_s, kp_s = _problem_for(rec, screen_ligs[:n_sub], dev, "f32")
@@ -539,17 +540,25 @@ def full_screen(rec, train_ligs, screen_ligs, variant, device="cuda", chains=32,
     kp_s.run_mc(cl, ci, cur, ce, best, be, True, ref_steps, cfg_r["bfgs_iters"], cfg_r["mc_temperature"],
                 cfg_r["mc_amp_pos"], cfg_r["mc_amp_rot"], seed + 5, 0)
     e_ref = _best_per_ligand(be, n_sub, chains)
-    floor = torch.minimum(torch.minimum(e_ref, e_l[:n_sub]), e_p[:n_sub])
-    for e, row in ((e_l, row_l), (e_p, row_p)):
+    floor = torch.minimum(e_ref, e_p[:n_sub])
+    for e, _ in learned:
+        floor = torch.minimum(floor, e[:n_sub])
+    for e, row in learned + [(e_p, row_p)]:
         gap = (e[:n_sub] - floor).cpu()
         row.update(median_gap=float(gap.median()), mean_gap=float(gap.mean()))
     torch.cuda.synchronize(dev)
-    return {"ligands": L, "chains": chains, "gap_subset": n_sub, "ref_steps": ref_steps, "train_ligands": len(train_ligs),
-            "train": train_rec, "train_ms": t_train[0].elapsed_time(t_train[1]), "learned_variant": {
-                "name": name, "prop_k": k, "prop_frac": frac, "target": tgt, "tries": tries, "hint": hint},
-            "learned_f16": row_l, "plain_f32": row_p,
-            "speedup_ligands_per_s": row_l["ligands_per_s"] / row_p["ligands_per_s"],
-            "both_within_gap_0.1": row_l["median_gap"] <= 0.1 and row_p["median_gap"] <= 0.1}
+    rows_l = [r for _, r in learned]
+    at_plain = interp_to_gap(rows_l, row_p["median_gap"])
+    at_bar = interp_to_gap(rows_l, 0.1)
+    out = {"ligands": L, "chains": chains, "gap_subset": n_sub, "ref_steps": ref_steps,
+           "train_ligands": len(train_ligs), "train": train_rec, "train_ms": t_train[0].elapsed_time(t_train[1]),
+           "learned_variant": {"name": name, "prop_k": k, "prop_frac": frac, "target": tgt, "tries": tries,
+                               "hint": hint},
+           "learned_f16": rows_l, "plain_f32": row_p,
+           "learned_at_plain_gap": at_plain, "learned_at_gap_0.1": at_bar}
+    if at_plain:
+        out["speedup_at_equal_gap"] = at_plain["ligands_per_s"] / row_p["ligands_per_s"]
+    return out
 
 
 def interp_to_gap(rows, gap):
@@ -579,12 +588,19 @@ def run_mc_segments(kp, net, chain_lig, chain_id, cur, cur_e, best, best_e, cfg,
     lowest-energy one."""
     steps = cfg["mc_steps"]
     pst = torch.zeros(4, dtype=torch.int64, device=kp.device)
+    marks = []   # per segment: events before the network launches and before the MC launch
     for sg in range(math.ceil(steps / prop_k)):
         k = min(prop_k, steps - sg * prop_k)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)] if stats is not None else None
+        if ev:
+            ev[0].record()
         hint = kp.prop_hint(chain_lig, best, best_e) if net.uses_hint and sg > 0 else None
         feat = kp.prop_features(chain_lig, cur, cur_e, hint)
         out = net.forward(feat)
         moves = kp.prop_sample(chain_lig, chain_id, out, cur, k * prop_tries, seed ^ 0x5EEDBA5E, sg)
+        if ev:
+            ev[1].record()
+            marks.append(ev)
         kp.run_mc(chain_lig, chain_id, cur, cur_e, best, best_e, init_opt and sg == 0, k, cfg["bfgs_iters"],
                   cfg["mc_temperature"], cfg["mc_amp_pos"], cfg["mc_amp_rot"], seed, sg * prop_k, prop=moves,
                   prop_stats=pst, prop_frac=prop_frac, log=log, prop_tries=prop_tries, hint=hint)
@@ -592,4 +608,12 @@ def run_mc_segments(kp, net, chain_lig, chain_id, cur, cur_e, best, best_e, cfg,
     if stats is not None:
         p, pa, q, qa = pst.tolist()
         stats.update(prop_steps=p, prop_accepted=pa, plain_steps=q, plain_accepted=qa)
+        if marks:
+            end = torch.cuda.Event(enable_timing=True)
+            end.record()
+            end.synchronize()
+            net_ms = sum(a.elapsed_time(b) for a, b in marks)
+            total = marks[0][0].elapsed_time(end)
+            # the network's share of the learned search: features, the three GEMMs with their epilogues, sampling
+            stats.update(net_ms=net_ms, mc_segments_ms=total - net_ms, segments=len(marks))
     return pst

@@ -300,8 +300,17 @@ def ligand(n_heavy: int, n_rot: int, seed: int, min_nonbonded: float = 2.9, max_
     raise RuntimeError(f"could not grow a ligand with {n_heavy} atoms (seed {seed})")
 
 
-def ligand_set(n: int, heavy_range, rot_range, seed0: int = 0):
-    """Ligands from seeds seed0..seed0+n-1; sizes drawn uniformly from the inclusive ranges with the same seed."""
+def ligand_set(n: int, heavy_range, rot_range, seed0: int = 0, workers: int = 1):
+    """Ligands from seeds seed0..seed0+n-1; sizes drawn uniformly from the inclusive ranges with the same seed.
+    workers > 1: the seeds are split over that many processes (started with spawn, so a caller that has already
+    initialised CUDA can use it); every ligand depends on its seed alone, so the list is the same."""
+    if workers > 1 and n >= 4 * workers:
+        import multiprocessing as mp
+        per = -(-n // workers)
+        parts = [(min(per, n - a), tuple(heavy_range), tuple(rot_range), seed0 + a) for a in range(0, n, per)]
+        with mp.get_context("spawn").Pool(len(parts)) as pool:
+            chunks = pool.starmap(ligand_set, parts)
+        return [x for c in chunks for x in c]
     out = []
     for s in range(seed0, seed0 + n):
         r = np.random.default_rng(10_000 + s)

@@ -74,7 +74,8 @@ def _args():
                          "the 8,000-atom receptor docked in one batch by the learned FP16 search and by the plain FP32 "
                          "search, gaps on a subset, the reference's CPU search on a sample")
     ap.add_argument("--screen-full-ligands", type=int, default=16384)
-    ap.add_argument("--screen-full-learned-steps", type=int, default=500)
+    ap.add_argument("--screen-full-learned-steps", default="400,600",
+                    help="budgets of the learned search (comma separated), interpolated to the plain run's gap")
     ap.add_argument("--screen-full-plain-steps", type=int, default=3000)
     ap.add_argument("--screen-full-subset", type=int, default=1024, help="ligands whose gap is measured")
     ap.add_argument("--screen-full-cpu", type=int, default=16,
@@ -432,6 +433,9 @@ def _learned_section(dev, n_train, n_eval):
         return {"steps": r["steps"], "ligands_per_s": r["ligands_per_s"], "evals_per_s": near["evals_per_s"]}
 
     plain, learned = at_bar("plain_f32"), at_bar("learned_f16")
+    # the network's share of the learned search (features, GEMMs, sampling vs the MC launches), over its budgets
+    lr = [r for r in ab["methods"]["learned_f16"] if "net_ms" in r]
+    net_share = (sum(r["net_ms"] for r in lr) / sum(r["net_ms"] + r["mc_segments_ms"] for r in lr)) if lr else None
     return {"workload": (f"screening shapes: 8000-atom receptor, 30 A box, 81^3 x 8 maps; {n_eval} held-out ligands "
                          f"(8-80 heavy atoms, 0-20 torsions) x 32 chains; proposal trained on {n_train} fresh "
                          f"ligands (2 self-training rounds)"),
@@ -439,7 +443,7 @@ def _learned_section(dev, n_train, n_eval):
             "speedup_ligands_per_s_at_gap_0.1": (learned["ligands_per_s"] / plain["ligands_per_s"]
                                                  if plain and learned else None),
             "train_ms": {k: v["train_ms"] for k, v in ab["train"].items() if isinstance(v, dict)},
-            "train_moves": ab["train"]["moves"], "wall_s": wall,
+            "train_moves": ab["train"]["moves"], "wall_s": wall, "network_share_of_learned_search": net_share,
             "rows": {m: [{k: r[k] for k in ("steps", "median_gap", "mean_gap", "ligands_per_s", "evals_per_s")}
                          for r in rs] for m, rs in ab["methods"].items()}}
 
@@ -525,15 +529,17 @@ def run_screen_full(args):
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
     rec2 = synth.config_receptor(2)
-    train = synth.ligand_set(args.screen_train, (8, 80), (0, 20), seed0=300_000)
-    ligs = synth.ligand_set(args.screen_full_ligands, (8, 80), (0, 20), seed0=700_000)
+    nw = min(16, os.cpu_count() or 1)     # the generator is Python; the seeds are split over processes
+    train = synth.ligand_set(args.screen_train, (8, 80), (0, 20), seed0=300_000, workers=nw)
+    ligs = synth.ligand_set(args.screen_full_ligands, (8, 80), (0, 20), seed0=700_000, workers=nw)
     variant = next(v for v in args.screen_variants.split(",") if v)
     f = variant.split(":")
     variant = (f[0], int(f[1]), float(f[2])) + ((f[3],) if len(f) > 3 else ()) + \
         ((int(f[4]),) if len(f) > 4 else ()) + ((f[5] in ("1", "hint"),) if len(f) > 5 else ())
     clocks = ClockSampler(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0])
     t0 = time.perf_counter()
-    res = full_screen(rec2, train, ligs, variant, device=dev, learned_steps=args.screen_full_learned_steps,
+    steps_l = tuple(int(x) for x in args.screen_full_learned_steps.split(",") if x)
+    res = full_screen(rec2, train, ligs, variant, device=dev, learned_steps=steps_l,
                       plain_steps=args.screen_full_plain_steps, n_sub=args.screen_full_subset,
                       log_cap=args.screen_log_cap)
     res["wall_s"] = time.perf_counter() - t0
