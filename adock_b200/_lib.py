@@ -79,13 +79,13 @@ _SIGS = {
     "adock_mc_noalloc": ([SP(Ligands), SP(Grids), SP(SF), SP(Receptors), SP(McArgs), P], I),
     "adock_prop_features": ([SP(Ligands), SP(Work), SP(Grids), SP(SF), P, I, P, P, P, P, P], I),
     "adock_prop_hint": ([I, I, P, P, I, P, P, P, P], I),
-    "adock_prop_sample": ([SP(Ligands), SP(Work), P, P, I, P, P, I, I, ctypes.c_ulonglong, I, P, P], I),
+    "adock_prop_sample": ([SP(Ligands), SP(Work), P, P, I, P, P, I, I, I, ctypes.c_ulonglong, I, P, P], I),
     "adock_gemm_bf16": ([I, I, I, P, ctypes.c_longlong, ctypes.c_longlong, P, ctypes.c_longlong, ctypes.c_longlong, P,
                          ctypes.c_longlong, F, P, I, P, P, ctypes.c_longlong, P], I),
     "adock_gemm_bf16_mma": ([I, I, I, P, ctypes.c_longlong, ctypes.c_longlong, P, ctypes.c_longlong,
                              ctypes.c_longlong, P, ctypes.c_longlong, F, P, I, P, P, ctypes.c_longlong, P], I),
     "adock_gemm_status": ([], I),
-    "adock_mlp_nll": ([P, P, I, P, P, P], I),
+    "adock_mlp_nll": ([P, P, I, I, P, P, P], I),
     "adock_silu_backward": ([P, P, ctypes.c_longlong, P, P], I),
     "adock_bias_grad": ([P, I, I, P, P], I),
     "adock_adam": ([P, P, P, P, P, ctypes.c_longlong, F, F, F, F, I, F, P], I),

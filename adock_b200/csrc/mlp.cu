@@ -315,8 +315,14 @@ __global__ void __launch_bounds__(128) gemm_bf16_tc_kernel(const __grid_constant
 
 // Gaussian NLL over the move dimensions: out [B, 64] (mu = out[:, 0:26], log_sigma = out[:, 32:58] clamped to
 // [-4, 2]); target [B, 32] (move in 0..25, torsion count in 26); rows of the batch weighted equally.
+// n_comp = 3: the translation is a mixture of 3 Gaussians with the shared per-axis sigma (out[:, 32:35]), means at
+// columns 0, 27, 58 (3 each) and mixing logits at columns 26, 30, 61; its term is
+// -log sum_k softmax(logits)_k N(t | mu_k, sigma). Rotation and torsions stay single Gaussians.
 // Writes dOut (BF16, [B, 64]) = d(mean loss)/d(out) and accumulates the loss sum into *loss.
-__global__ void nll_kernel(const float* __restrict__ out, const float* __restrict__ target, int B,
+__constant__ int MIX_MEAN[3] = {0, 27, 58};
+__constant__ int MIX_LOGIT[3] = {26, 30, 61};
+
+__global__ void nll_kernel(const float* __restrict__ out, const float* __restrict__ target, int B, int n_comp,
                            __nv_bfloat16* __restrict__ dout, float* __restrict__ loss) {
     const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (row >= B) return;
@@ -324,9 +330,10 @@ __global__ void nll_kernel(const float* __restrict__ out, const float* __restric
     const float* t = target + (long long)row * 32;
     const int nt = (int)t[26];
     const float inv = 1.f / (float)B;
+    const bool mix = n_comp > 1;
     float l = 0.f, dmu = 0.f, dls = 0.f;
     const int d = lane;
-    const bool active = d < 26 && (d < 6 || d - 6 < nt);
+    const bool active = d < 26 && (d < 6 || d - 6 < nt) && !(mix && d < 3);
     if (active) {
         const float mu = o[d], ls_raw = o[32 + d];
         const float ls = fminf(fmaxf(ls_raw, -4.f), 2.f);
@@ -337,6 +344,47 @@ __global__ void nll_kernel(const float* __restrict__ out, const float* __restric
     }
     dout[(long long)row * 64 + lane] = __float2bfloat16(dmu);
     dout[(long long)row * 64 + 32 + lane] = __float2bfloat16(dls);
+    if (mix) {
+        __syncwarp();
+        if (lane == 0) {   // the translation mixture: overwrites its columns after the per-lane defaults (0)
+            float ls[3], isd[3], lg[3], lp[3], z[3][3];
+            for (int a = 0; a < 3; ++a) {
+                ls[a] = fminf(fmaxf(o[32 + a], -4.f), 2.f);
+                isd[a] = __expf(-ls[a]);
+            }
+            float mg = -3.4e38f, mp = -3.4e38f;
+            for (int k = 0; k < 3; ++k) {
+                lg[k] = o[MIX_LOGIT[k]];
+                lp[k] = lg[k];
+                for (int a = 0; a < 3; ++a) {
+                    z[k][a] = (t[a] - o[MIX_MEAN[k] + a]) * isd[a];
+                    lp[k] -= 0.5f * z[k][a] * z[k][a];
+                }
+                mg = fmaxf(mg, lg[k]);
+                mp = fmaxf(mp, lp[k]);
+            }
+            float sg = 0.f, sp = 0.f;
+            for (int k = 0; k < 3; ++k) {
+                sg += __expf(lg[k] - mg);
+                sp += __expf(lp[k] - mp);
+            }
+            const float lse_g = mg + __logf(sg), lse_p = mp + __logf(sp);
+            l += lse_g - lse_p + ls[0] + ls[1] + ls[2];
+            float dl[3] = {0.f, 0.f, 0.f};
+            for (int k = 0; k < 3; ++k) {
+                const float r = __expf(lp[k] - lse_p), p = __expf(lg[k] - lse_g);
+                dout[(long long)row * 64 + MIX_LOGIT[k]] = __float2bfloat16((p - r) * inv);
+                for (int a = 0; a < 3; ++a) {
+                    dout[(long long)row * 64 + MIX_MEAN[k] + a] = __float2bfloat16(-r * z[k][a] * isd[a] * inv);
+                    dl[a] += r * (1.f - z[k][a] * z[k][a]);
+                }
+            }
+            for (int a = 0; a < 3; ++a) {
+                const float raw = o[32 + a];
+                dout[(long long)row * 64 + 32 + a] = __float2bfloat16((raw > -4.f && raw < 2.f) ? dl[a] * inv : 0.f);
+            }
+        }
+    }
     l = warp_sum(l);
     if (lane == 0) atomicAdd(loss, l);
 }
@@ -463,10 +511,12 @@ extern "C" int adock_gemm_status(void) {
     return ADOCK_OK;
 }
 
-extern "C" int adock_mlp_nll(const float* out, const float* target, int B, void* dout, float* loss, void* stream) {
+extern "C" int adock_mlp_nll(const float* out, const float* target, int B, int n_comp, void* dout, float* loss,
+                             void* stream) {
     ADOCK_CHECK_ARG(out && target && dout && loss && B >= 0, "bad argument");
+    ADOCK_CHECK_ARG(n_comp == 1 || n_comp == 3, "n_comp must be 1 or 3 (got %d)", n_comp);
     if (B == 0) return ADOCK_OK;
-    nll_kernel<<<(B + 3) / 4, 128, 0, (cudaStream_t)stream>>>(out, target, B, (__nv_bfloat16*)dout, loss);
+    nll_kernel<<<(B + 3) / 4, 128, 0, (cudaStream_t)stream>>>(out, target, B, n_comp, (__nv_bfloat16*)dout, loss);
     ADOCK_CUDA(cudaGetLastError());
     return ADOCK_OK;
 }

@@ -209,8 +209,8 @@ __global__ void __launch_bounds__(256) neighbours_kernel(const __grid_constant__
 // to the chain's state: t + d[0:3], exp(d[3:6]) q, theta + d[6:26] below the torsion count (theta kept above it).
 // The floors on the spread (0.5 A, 0.25 rad, 0.5 rad) keep the proposals exploring.
 __global__ void prop_sample_kernel(const int4* info, const int* chain_lig, const int* chain_id, int n,
-                                   const float* out, const float* state, int SD, int k, unsigned long long seed,
-                                   int segment, float* targets) {
+                                   const float* out, const float* state, int SD, int k, int n_comp,
+                                   unsigned long long seed, int segment, float* targets) {
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (long long)n * k) return;
     const int kk = (int)(idx % k);
@@ -231,6 +231,16 @@ __global__ void prop_sample_kernel(const int4* info, const int* chain_lig, const
             const float floor_sd = j < 3 ? 0.5f : (j < 6 ? 0.25f : 0.5f);
             d[j] = o[j] + fmaxf(__expf(ls), floor_sd) * z;
         }
+    }
+    if (n_comp == 3) {
+        // translation mixture: component by its softmax weight (mean columns 0, 27, 58; logits 26, 30, 61), the
+        // same standard-normal draws and spread as the single Gaussian
+        const float g0 = o[26], g1 = o[30], g2 = o[61];
+        const float m = fmaxf(g0, fmaxf(g1, g2));
+        const float w0 = __expf(g0 - m), w1 = __expf(g1 - m), w2 = __expf(g2 - m);
+        const float u = uniform01(seed, cid, step, 52) * (w0 + w1 + w2);
+        const int mc = u < w0 ? 0 : (u < w0 + w1 ? 27 : 58);
+        for (int j = 0; j < 3; ++j) d[j] += o[mc + j] - o[j];
     }
     float* y = targets + idx * PROP_MOVE;
     y[0] = s[0] + d[0]; y[1] = s[1] + d[1]; y[2] = s[2] + d[2];
@@ -612,16 +622,18 @@ extern "C" int adock_prop_hint(int L, int n, const int* chain_lig, const float* 
 
 extern "C" int adock_prop_sample(const adock_ligands_t* lig, const adock_work_t* work, const int* chain_lig,
                                  const int* chain_id, int n, const float* net_out, const float* state, int SD, int k,
-                                 unsigned long long seed, int segment, float* targets, void* stream) {
+                                 int n_comp, unsigned long long seed, int segment, float* targets, void* stream) {
     ADOCK_CHECK_ARG(lig && work && work->info, "null argument");
     ADOCK_CHECK_ARG(n >= 0 && k >= 1 && k <= 512, "n must be >= 0 and k in [1, 512]");
+    ADOCK_CHECK_ARG(n_comp == 1 || n_comp == 3, "n_comp must be 1 or 3 (got %d)", n_comp);
     ADOCK_CHECK_ARG(SD >= 7, "SD must be >= 7");
     if (n == 0) return ADOCK_OK;
     ADOCK_CHECK_ARG(chain_lig && chain_id && net_out && state && targets, "null array argument");
     const long long total = (long long)n * k;
     const unsigned blocks = (unsigned)((total + 127) / 128);
     prop_sample_kernel<<<blocks, 128, 0, (cudaStream_t)stream>>>((const int4*)work->info, chain_lig, chain_id, n,
-                                                                 net_out, state, SD, k, seed, segment, targets);
+                                                                 net_out, state, SD, k, n_comp, seed, segment,
+                                                                 targets);
     ADOCK_CUDA(cudaGetLastError());
     return ADOCK_OK;
 }

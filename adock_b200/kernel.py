@@ -170,7 +170,7 @@ class B200KernelProblem:
                       _lib.ptr(keys), _lib.ptr(hint), _lib.stream_ptr())
         return hint
 
-    def prop_sample(self, chain_lig, chain_id, net_out, state, k, seed, segment):
+    def prop_sample(self, chain_lig, chain_id, net_out, state, k, seed, segment, n_comp=1):
         """Target states [N, k, 32] (t, q, torsions 0..19) drawn from the network's Gaussian (net_out [N, 64]) over
         moves from the states state [N, SD] the network read."""
         N = net_out.shape[0]
@@ -181,7 +181,8 @@ class B200KernelProblem:
         assert st.shape == (N, self.SD)
         with torch.cuda.device(self.device):
             _lib.call("adock_prop_sample", self.c_lig, self.c_work, _lib.ptr(cl), _lib.ptr(ci), N, _lib.ptr(no),
-                      _lib.ptr(st), self.SD, int(k), int(seed) & 0xFFFFFFFFFFFFFFFF, int(segment), _lib.ptr(targets),
+                      _lib.ptr(st), self.SD, int(k), int(n_comp), int(seed) & 0xFFFFFFFFFFFFFFFF, int(segment),
+                      _lib.ptr(targets),
                       _lib.stream_ptr())
         return targets
 

@@ -48,12 +48,19 @@ class ProposalNet:
     """320 -> 256 -> 256 -> 64 MLP; weights W_i stored [K, N] row-major (x @ W). uses_hint: the network reads the
     ligand-best hint columns (else they are 0 in its inputs)."""
 
-    def __init__(self, device="cuda", seed=0, init_log_sd=(0.0, -1.0, -0.5), uses_hint=False):
+    def __init__(self, device="cuda", seed=0, init_log_sd=(0.0, -1.0, -0.5), uses_hint=False, n_comp=1):
         dev = torch.device(device)
         g = torch.Generator(device="cpu").manual_seed(seed)
         dims = [(IN, HID), (HID, HID), (HID, OUT)]
         self.W = [(torch.randn(k, n, generator=g) * math.sqrt(2.0 / k)).to(dev) for k, n in dims]
         self.W[2].mul_(0.01)
+        self.n_comp = int(n_comp)
+        assert self.n_comp in (1, 3)
+        if self.n_comp == 3:
+            # translation mixture: the extra means (columns 27-29, 58-60) start further apart than the 0.01 scale
+            # of the other outputs, so that the components can take different basins
+            for c in (27, 28, 29, 58, 59, 60):
+                self.W[2][:, c] *= 30.0
         self.b = [torch.zeros(n, device=dev) for _, n in dims]
         # initial spread: log sd for translation, rotation, torsion columns
         self.b[2][32:35] = init_log_sd[0]
@@ -69,7 +76,7 @@ class ProposalNet:
 
     def state_dict(self):
         return {"W": [w.cpu() for w in self.W], "b": [b.cpu() for b in self.b], "step": self.step,
-                "uses_hint": self.uses_hint}
+                "uses_hint": self.uses_hint, "n_comp": self.n_comp}
 
     def load_state_dict(self, d):
         for dst, src in zip(self.W + self.b, d["W"] + d["b"]):
@@ -77,6 +84,7 @@ class ProposalNet:
         self.Wb = [w.to(torch.bfloat16).contiguous() for w in self.W]
         self.step = int(d.get("step", 0))
         self.uses_hint = bool(d.get("uses_hint", False))
+        self.n_comp = int(d.get("n_comp", 1))
 
     def forward(self, x, save=False):
         """x: BF16 [B, 320] -> out FP32 [B, 64] (and saved activations when save)."""
@@ -112,7 +120,7 @@ class ProposalNet:
         dA1 = torch.empty(B, HID, dtype=torch.bfloat16, device=dev)
         s = _lib.stream_ptr
         with torch.cuda.device(dev):
-            _lib.call("adock_mlp_nll", _lib.ptr(out), _lib.ptr(y), B, _lib.ptr(dout), _lib.ptr(loss), s())
+            _lib.call("adock_mlp_nll", _lib.ptr(out), _lib.ptr(y), B, self.n_comp, _lib.ptr(dout), _lib.ptr(loss), s())
             # layer 3: dW3 = h2^T dout, db3, dH2 = dout W3^T
             _gemm(h2, (1, HID), dout, (OUT, 1), HID, OUT, B, C=gW[2])
             _lib.call("adock_bias_grad", _lib.ptr(dout), B, OUT, _lib.ptr(gb[2]), s())
@@ -305,11 +313,12 @@ def _best_per_ligand(best_e, L, M):
 
 def parse_learned(learned):
     """Learned variants (name, segment steps, learned fraction[, training "chain" | "ligand" | "dagger" |
-    "daggerN"[, tries[, hint]]]) -> {name: (prop_k, prop_frac, target, tries, hint)}: the chain's or the ligand's
-    best pose as target, or the chain network fine-tuned N times on its own search's moves; tries candidate
-    targets per learned step; hint: the network reads the ligand-best hint."""
+    "daggerN"[, tries[, hint[, n_comp]]]]) -> {name: (prop_k, prop_frac, target, tries, hint, n_comp)}: the
+    chain's or the ligand's best pose as target, or the chain network fine-tuned N times on its own search's
+    moves; tries candidate targets per learned step; hint: the network reads the ligand-best hint; n_comp: 1, or 3
+    for a translation mixture."""
     return {v[0]: (v[1], v[2], v[3] if len(v) > 3 else "chain", int(v[4]) if len(v) > 4 else 1,
-                   bool(v[5]) if len(v) > 5 else False) for v in learned}
+                   bool(v[5]) if len(v) > 5 else False, int(v[6]) if len(v) > 6 else 1) for v in learned}
 
 
 def _rounds(t):   # "dagger" = 1 self-training round on top of "chain", "dagger2" = 2, ...
@@ -336,38 +345,43 @@ def train_variants(rec, train_ligs, variants, device="cuda", chains=32, train_st
     best = cur.clone()
     ce, be = torch.zeros(N, device=dev), torch.full((N,), float("inf"), device=dev)
     torch.cuda.synchronize(dev)
-    any_hint = any(h for (_, _, _, _, h) in variants)
+    any_hint = any(v[4] for v in variants)
     X, Yc, Yl = collect(kp_t, cl, ci, cur, ce, best, be, cfg_tr, seed=seed + 1, cap=log_cap, target="both",
                         hint_segment=32 if any_hint else 0)
     nets = {}
     rec_out = {"moves": int(X.shape[0]), "epochs": epochs}
-    targets = {(t, h) for (_, _, t, _, h) in variants}
-    for (t, h) in list(targets):
+    # one network family per (hint, n_comp); each family trains the rounds its targets need
+    targets = {(v[2], v[4], v[5]) for v in variants}
+    for (t, h, m) in list(targets):
         for n in range(_rounds(t)):
-            targets.add((_dagger_name(n), h))
-    for (tgt, hint) in sorted(targets, key=lambda th: (th[1], th[0] == "ligand", _rounds(th[0]))):
+            targets.add((_dagger_name(n), h, m))
+
+    def label(tgt, hint, mix):
+        return tgt + ("_hint" if hint else "") + ("_mix3" if mix > 1 else "")
+
+    for (tgt, hint, mix) in sorted(targets, key=lambda th: (th[1], th[2], th[0] == "ligand", _rounds(th[0]))):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         n = _rounds(tgt)
         if n > 0:
             # self-training round n: the previous round's network drives the search on the training ligands with
             # the log on; a copy of it is fine-tuned on those moves (targets: that search's own final minima)
-            prev = nets[(_dagger_name(n - 1), hint)]
-            net = ProposalNet(dev, seed=seed, uses_hint=hint)
+            prev = nets[(_dagger_name(n - 1), hint, mix)]
+            net = ProposalNet(dev, seed=seed, uses_hint=hint, n_comp=mix)
             net.load_state_dict(prev.state_dict())
             cl2, ci2, cur2 = _starts(prob_t, kp_t, cfg_tr, seed + 5 * n)
             X2, Y2 = collect_learned(kp_t, prev, cl2, ci2, cur2, cfg_tr, seed + 5 * n + 1, log_cap)
             loss = net.fit(X2, Y2, epochs=epochs, batch=4096, lr=5e-4, seed=seed + n, log=log)
-            rec_out[f"{tgt}{'_hint' if hint else ''}_moves"] = int(X2.shape[0])
+            rec_out[label(tgt, hint, mix) + "_moves"] = int(X2.shape[0])
             del X2, Y2
         else:
             Y = Yc if tgt == "chain" else Yl
-            net = ProposalNet(dev, seed=seed, uses_hint=hint)
+            net = ProposalNet(dev, seed=seed, uses_hint=hint, n_comp=mix)
             loss = net.fit(X if hint else without_hint(X), Y, epochs=epochs, batch=4096, lr=1e-3, seed=seed, log=log)
         e1.record()
         torch.cuda.synchronize(dev)
-        nets[(tgt, hint)] = net
-        rec_out[tgt + ("_hint" if hint else "")] = {"final_loss": loss, "train_ms": e0.elapsed_time(e1)}
+        nets[(tgt, hint, mix)] = net
+        rec_out[label(tgt, hint, mix)] = {"final_loss": loss, "train_ms": e0.elapsed_time(e1)}
     return nets, rec_out
 
 
@@ -412,8 +426,8 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
         ce, be = torch.zeros(cur.shape[0], device=dev), torch.full((cur.shape[0],), float("inf"), device=dev)
         st = {}
         if method in variants:
-            k, frac, tgt, tries, hint = variants[method]
-            run_mc_segments(kp, nets[(tgt, hint)], cl, ci, cur, ce, best, be, cfg, seed + 3, prop_k=k,
+            k, frac, tgt, tries, hint, mix = variants[method]
+            run_mc_segments(kp, nets[(tgt, hint, mix)], cl, ci, cur, ce, best, be, cfg, seed + 3, prop_k=k,
                             prop_frac=frac, stats=st, prop_tries=tries)
         else:
             kp.run_mc(cl, ci, cur, ce, best, be, True, steps, cfg["bfgs_iters"], cfg["mc_temperature"],
@@ -427,8 +441,8 @@ def ab_compare(rec, train_ligs, eval_ligs, device="cuda", chains=32, budgets=(12
 
     ref, ref_ms, ref_st = run("plain_f32", ref_steps)
     results = {}
-    out["learned_variants"] = {n: {"prop_k": k, "prop_frac": f, "target": t, "tries": r, "hint": h}
-                               for n, (k, f, t, r, h) in variants.items()}
+    out["learned_variants"] = {n: {"prop_k": k, "prop_frac": f, "target": t, "tries": r, "hint": h, "n_comp": m}
+                               for n, (k, f, t, r, h, m) in variants.items()}
     for m in ("plain_f32", *(("plain_f16",) if plain_f16 else ()), *variants):
         for S in (learned_budgets or budgets if m in variants else budgets):
             results[(m, S)] = run(m, S)
@@ -485,13 +499,13 @@ def full_screen(rec, train_ligs, screen_ligs, variant, device="cuda", chains=32,
     from . import params
     dev = torch.device(device)
     v = parse_learned([variant])
-    name, (k, frac, tgt, tries, hint) = next(iter(v.items()))
+    name, (k, frac, tgt, tries, hint, mix) = next(iter(v.items()))
     t_train = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t_train[0].record()
     nets, train_rec = train_variants(rec, train_ligs, v.values(), dev, chains=chains, train_steps=train_steps,
                                      log_cap=log_cap, epochs=epochs, seed=seed, log=log)
     t_train[1].record()
-    net = nets[(tgt, hint)]
+    net = nets[(tgt, hint, mix)]
     del nets
     L = len(screen_ligs)
     n_sub = min(n_sub, L)
@@ -553,7 +567,7 @@ def full_screen(rec, train_ligs, screen_ligs, variant, device="cuda", chains=32,
     out = {"ligands": L, "chains": chains, "gap_subset": n_sub, "ref_steps": ref_steps,
            "train_ligands": len(train_ligs), "train": train_rec, "train_ms": t_train[0].elapsed_time(t_train[1]),
            "learned_variant": {"name": name, "prop_k": k, "prop_frac": frac, "target": tgt, "tries": tries,
-                               "hint": hint},
+                               "hint": hint, "n_comp": mix},
            "learned_f16": rows_l, "plain_f32": row_p,
            "learned_at_plain_gap": at_plain, "learned_at_gap_0.1": at_bar}
     if at_plain:
@@ -597,7 +611,7 @@ def run_mc_segments(kp, net, chain_lig, chain_id, cur, cur_e, best, best_e, cfg,
         hint = kp.prop_hint(chain_lig, best, best_e) if net.uses_hint and sg > 0 else None
         feat = kp.prop_features(chain_lig, cur, cur_e, hint)
         out = net.forward(feat)
-        moves = kp.prop_sample(chain_lig, chain_id, out, cur, k * prop_tries, seed ^ 0x5EEDBA5E, sg)
+        moves = kp.prop_sample(chain_lig, chain_id, out, cur, k * prop_tries, seed ^ 0x5EEDBA5E, sg, net.n_comp)
         if ev:
             ev[1].record()
             marks.append(ev)

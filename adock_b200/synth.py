@@ -305,11 +305,14 @@ def ligand_set(n: int, heavy_range, rot_range, seed0: int = 0, workers: int = 1)
     workers > 1: the seeds are split over that many processes (started with spawn, so a caller that has already
     initialised CUDA can use it); every ligand depends on its seed alone, so the list is the same."""
     if workers > 1 and n >= 4 * workers:
+        # a pool that fails to start its workers (e.g. a caller script without a __main__ guard, which spawned
+        # workers re-import) raises BrokenProcessPool instead of waiting for them
         import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
         per = -(-n // workers)
         parts = [(min(per, n - a), tuple(heavy_range), tuple(rot_range), seed0 + a) for a in range(0, n, per)]
-        with mp.get_context("spawn").Pool(len(parts)) as pool:
-            chunks = pool.starmap(ligand_set, parts)
+        with ProcessPoolExecutor(len(parts), mp_context=mp.get_context("spawn")) as pool:
+            chunks = list(pool.map(ligand_set, *zip(*parts)))
         return [x for c in chunks for x in c]
     out = []
     for s in range(seed0, seed0 + n):

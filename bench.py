@@ -59,7 +59,8 @@ def _args():
     ap.add_argument("--ab-eval", type=int, default=256, help="held-out ligands for the A/B comparison")
     ap.add_argument("--ab-variants", default="learned_f16:32:0.3",
                     help="learned variants name:segment_steps:learned_fraction[:chain|ligand|dagger training[:tries"
-                         "[:hint]]], comma separated (hint: the network reads the ligand-best hint)")
+                         "[:hint[:n_comp]]]], comma separated (hint: the network reads the ligand-best hint; n_comp 3: "
+                         "translation mixture)")
     ap.add_argument("--screen", action="store_true",
                     help="screening comparison on the 8,000-atom receptor with 8-80-atom ligands (FP16 + learned "
                          "proposal vs plain FP32 at equal median gap)")
@@ -374,7 +375,8 @@ def run_ours(args, rank, world, local_rank):
         for v in spec.split(","):
             f = v.split(":")
             out_v.append((f[0], int(f[1]), float(f[2])) + ((f[3],) if len(f) > 3 else ())
-                         + ((int(f[4]),) if len(f) > 4 else ()) + ((f[5] in ("1", "hint"),) if len(f) > 5 else ()))
+                         + ((int(f[4]),) if len(f) > 4 else ()) + ((f[5] in ("1", "hint"),) if len(f) > 5 else ())
+                         + ((int(f[6]),) if len(f) > 6 else ()))
         return out_v
 
     variants = parse_variants(args.ab_variants)
@@ -535,7 +537,8 @@ def run_screen_full(args):
     variant = next(v for v in args.screen_variants.split(",") if v)
     f = variant.split(":")
     variant = (f[0], int(f[1]), float(f[2])) + ((f[3],) if len(f) > 3 else ()) + \
-        ((int(f[4]),) if len(f) > 4 else ()) + ((f[5] in ("1", "hint"),) if len(f) > 5 else ())
+        ((int(f[4]),) if len(f) > 4 else ()) + ((f[5] in ("1", "hint"),) if len(f) > 5 else ()) + \
+        ((int(f[6]),) if len(f) > 6 else ())
     clocks = ClockSampler(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0])
     t0 = time.perf_counter()
     steps_l = tuple(int(x) for x in args.screen_full_learned_steps.split(",") if x)

@@ -294,10 +294,11 @@ int adock_prop_hint(int L, int n, const int* chain_lig, const float* best, int S
  * around the states state [n, SD] the network read: move = mean + max(exp(log_sd), floor) * z, z standard normal
  * from a counter-based stream of (seed, chain_id, segment, slot), applied to the state (translation added,
  * rotation vector composed on the left of q, torsion deltas added; torsions past a ligand's count keep their
- * value). k <= 512. */
+ * value). k <= 512. n_comp = 3: the translation mean is one of the network's 3 mixture components (means at
+ * columns 0, 27, 58, mixing logits at 26, 30, 61), drawn by its softmax weight; n_comp = 1: column 0 only. */
 int adock_prop_sample(const adock_ligands_t* lig, const adock_work_t* work, const int* chain_lig, const int* chain_id,
-                      int n, const float* net_out, const float* state, int SD, int k, unsigned long long seed,
-                      int segment, float* targets, void* stream);
+                      int n, const float* net_out, const float* state, int SD, int k, int n_comp,
+                      unsigned long long seed, int segment, float* targets, void* stream);
 /* C[M,N] = A[M,K] B[K,N] on the 5th-generation tensor cores (tcgen05.mma, accumulator in tensor memory; BF16
  * operands at any strides, FP32 accumulation); epilogue C = acc + beta C + bias, optional pre-activation copy,
  * optional SiLU (act = 1), optional BF16 copy Cb. */
@@ -313,8 +314,8 @@ int adock_gemm_bf16_mma(int M, int N, int K, const void* A, long long sAm, long 
  * for its tensor-core work (its tile is then not written), else 0. Clears the status. */
 int adock_gemm_status(void);
 /* Gaussian NLL of moves target [B, 32] under out [B, 64]; dout (BF16 [B, 64]) = gradient of the batch mean;
- * *loss += summed NLL. */
-int adock_mlp_nll(const float* out, const float* target, int B, void* dout, float* loss, void* stream);
+ * *loss += summed NLL. n_comp = 3: the translation term is a 3-component mixture (layout as adock_prop_sample). */
+int adock_mlp_nll(const float* out, const float* target, int B, int n_comp, void* dout, float* loss, void* stream);
 /* dA = dH * SiLU'(A), BF16 output. */
 int adock_silu_backward(const float* dH, const float* A, long long n, void* dA, void* stream);
 /* db = column sums of dA (BF16 [rows, cols]). */

@@ -74,10 +74,11 @@ def test_gemm_tcgen05_epilogue_matches_mma_sync(dev, M, N, K):
     torch.testing.assert_close(a, b, rtol=1e-5, atol=1e-4)
 
 
-def test_network_gradients_match_float64_oracle(dev):
+@pytest.mark.parametrize("n_comp", [1, 3])
+def test_network_gradients_match_float64_oracle(dev, n_comp):
     from oracle import mlp as O
     from adock_b200.proposal import ProposalNet
-    net = ProposalNet(dev, seed=3)
+    net = ProposalNet(dev, seed=3, n_comp=n_comp)
     for w in net.W:   # a non-trivial network
         w.add_(torch.randn_like(w) * 0.05)
     net.Wb = [w.to(torch.bfloat16).contiguous() for w in net.W]
@@ -91,7 +92,7 @@ def test_network_gradients_match_float64_oracle(dev):
     loss, grads = net.loss_grad(X, Y)
     Wr = [w.to(torch.bfloat16).double().cpu().numpy() for w in net.W]
     lo, go = O.loss_and_grads(Wr, [b.double().cpu().numpy() for b in net.b], X.double().cpu().numpy(),
-                              Y.double().cpu().numpy())
+                              Y.double().cpu().numpy(), n_comp=n_comp)
     assert abs(float(loss) - lo) <= 1e-2 * max(1.0, abs(lo))
     for gg, gr in zip(grads, go):
         gg = gg.double().cpu().numpy()

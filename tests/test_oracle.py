@@ -142,3 +142,29 @@ def test_receptor_min_separation():
     assert d[:, 1].min() >= 2.8 - 1e-3
     assert len(rec["rec_xyz"]) == 1500
     assert rec["rec_xyz"].min() >= 0 and rec["rec_xyz"].max() <= 40.0
+
+
+@pytest.mark.parametrize("n_comp", [1, 3])
+def test_mlp_oracle_gradient_matches_finite_differences(n_comp):
+    """The float64 network oracle (the yardstick of the GPU training kernels): its analytic gradients of the
+    output-layer bias, including the translation mixture's means, logits and shared spreads, against central
+    differences of its own loss."""
+    from oracle import mlp as O
+    rng = np.random.default_rng(3)
+    dims = [(320, 16), (16, 16), (16, 64)]
+    W = [rng.normal(0, 0.3, d) for d in dims]
+    b = [rng.normal(0, 0.3, d[1]) for d in dims]
+    X = rng.normal(0, 1, (8, 320))
+    Y = rng.normal(0, 0.5, (8, 32))
+    Y[:, 26] = rng.integers(0, 21, 8)
+    Y[:, 27:] = 0
+    _, g = O.loss_and_grads(W, b, X, Y, n_comp=n_comp)
+    h = 1e-5
+    cols = [0, 1, 2, 3, 10, 26, 27, 30, 32, 33, 34, 40, 58, 60, 61]
+    for c in cols:
+        bp = [v.copy() for v in b]
+        bm = [v.copy() for v in b]
+        bp[2][c] += h
+        bm[2][c] -= h
+        fd = (O.loss_and_grads(W, bp, X, Y, n_comp=n_comp)[0] - O.loss_and_grads(W, bm, X, Y, n_comp=n_comp)[0]) / (2 * h)
+        assert abs(fd - g[5][c]) <= 1e-5 + 1e-4 * abs(fd), (c, fd, g[5][c])
