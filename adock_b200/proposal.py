@@ -592,6 +592,23 @@ def interp_to_gap(rows, gap):
     return None
 
 
+def frac_at(prop_frac, step):
+    """The learned-step fraction of the segment that starts at ``step``: a number, or (early, late, until)."""
+    if isinstance(prop_frac, (tuple, list)):
+        early, late, until = prop_frac
+        return float(early if step < until else late)
+    return float(prop_frac)
+
+
+def parse_frac(text):
+    """A learned-fraction field of a variant spec: "0.3", or "0.5>0.3@128" for 0.5 before step 128 and 0.3 after."""
+    if ">" in text:
+        a, rest = text.split(">")
+        b, c = rest.split("@")
+        return (float(a), float(b), int(c))
+    return float(text)
+
+
 def run_mc_segments(kp, net, chain_lig, chain_id, cur, cur_e, best, best_e, cfg, seed, prop_k=32, init_opt=True,
                     stats=None, prop_frac=0.3, log=None, prop_tries=1):
     """MC with learned proposals: the run is cut into segments of prop_k steps; before each segment the network
@@ -599,7 +616,8 @@ def run_mc_segments(kp, net, chain_lig, chain_id, cur, cur_e, best, best_e, cfg,
     step proposes the next of them with probability prop_frac, else it takes the plain random move (and plain MC
     after 8 consecutive rejections of learned proposals). log: the training-data log of run_mc, kept across the
     segments. prop_tries > 1: each learned step draws that many targets, evaluates each once and optimises the
-    lowest-energy one."""
+    lowest-energy one. prop_frac may be a schedule (early, late, until): the fraction ``early`` for the segments that
+    start before step ``until``, ``late`` after."""
     steps = cfg["mc_steps"]
     pst = torch.zeros(4, dtype=torch.int64, device=kp.device)
     marks = []   # per segment: events before the network launches and before the MC launch
@@ -617,7 +635,8 @@ def run_mc_segments(kp, net, chain_lig, chain_id, cur, cur_e, best, best_e, cfg,
             marks.append(ev)
         kp.run_mc(chain_lig, chain_id, cur, cur_e, best, best_e, init_opt and sg == 0, k, cfg["bfgs_iters"],
                   cfg["mc_temperature"], cfg["mc_amp_pos"], cfg["mc_amp_rot"], seed, sg * prop_k, prop=moves,
-                  prop_stats=pst, prop_frac=prop_frac, log=log, prop_tries=prop_tries, hint=hint)
+                  prop_stats=pst, prop_frac=frac_at(prop_frac, sg * prop_k), log=log, prop_tries=prop_tries,
+                  hint=hint)
     check_gemm("learned-proposal search")
     if stats is not None:
         p, pa, q, qa = pst.tolist()

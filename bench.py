@@ -370,11 +370,13 @@ def run_ours(args, rank, world, local_rank):
            "mc_autotune": __import__("adock_b200.autotune", fromlist=["cached"]).cached()}
     if rank == 0 and world == 1 and not args.no_extras:
         out["grid_and_precision"] = _grid_and_precision(dev, ligs)
+    from adock_b200.proposal import parse_frac
+
     def parse_variants(spec):
         out_v = []
         for v in spec.split(","):
             f = v.split(":")
-            out_v.append((f[0], int(f[1]), float(f[2])) + ((f[3],) if len(f) > 3 else ())
+            out_v.append((f[0], int(f[1]), parse_frac(f[2])) + ((f[3],) if len(f) > 3 else ())
                          + ((int(f[4]),) if len(f) > 4 else ()) + ((f[5] in ("1", "hint"),) if len(f) > 5 else ())
                          + ((int(f[6]),) if len(f) > 6 else ()))
         return out_v
@@ -527,7 +529,7 @@ def run_screen_full(args):
     import numpy as np
     import torch
     from adock_b200 import params, synth
-    from adock_b200.proposal import full_screen
+    from adock_b200.proposal import full_screen, parse_frac
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
     rec2 = synth.config_receptor(2)
@@ -536,7 +538,7 @@ def run_screen_full(args):
     ligs = synth.ligand_set(args.screen_full_ligands, (8, 80), (0, 20), seed0=700_000, workers=nw)
     variant = next(v for v in args.screen_variants.split(",") if v)
     f = variant.split(":")
-    variant = (f[0], int(f[1]), float(f[2])) + ((f[3],) if len(f) > 3 else ()) + \
+    variant = (f[0], int(f[1]), parse_frac(f[2])) + ((f[3],) if len(f) > 3 else ()) + \
         ((int(f[4]),) if len(f) > 4 else ()) + ((f[5] in ("1", "hint"),) if len(f) > 5 else ()) + \
         ((int(f[6]),) if len(f) > 6 else ())
     clocks = ClockSampler(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0])

@@ -83,3 +83,12 @@ def test_interp_to_gap():
     assert abs(1 / r["ligands_per_s"] - ((1 - w) / 100 + w / 50)) < 1e-12
     assert interp_to_gap(rows, 0.5) == {"steps": 500, "ligands_per_s": 100.0}
     assert interp_to_gap(rows, 0.001) is None
+
+
+def test_learned_fraction_schedule():
+    from adock_b200.proposal import frac_at, parse_frac
+    assert parse_frac("0.3") == 0.3
+    sched = parse_frac("0.5>0.3@128")
+    assert sched == (0.5, 0.3, 128)
+    assert [frac_at(sched, s) for s in (0, 96, 128, 500)] == [0.5, 0.5, 0.3, 0.3]
+    assert frac_at(0.3, 1000) == 0.3
