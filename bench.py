@@ -67,7 +67,7 @@ def _args():
     ap.add_argument("--screen-train", type=int, default=1536, help="fresh ligands for the screening proposal's training")
     ap.add_argument("--screen-eval", type=int, default=1024, help="held-out ligands of the screening comparison")
     ap.add_argument("--screen-log-cap", type=int, default=4_000_000, help="training moves kept per collection")
-    ap.add_argument("--screen-variants", default="learned_dagger2:32:0.3:dagger2:4:0:3",
+    ap.add_argument("--screen-variants", default="learned_dagger2:32:0.6>0.3@64:dagger2:4:0:3",
                     help="learned variants of the screening comparison (as --ab-variants; dagger, dagger2, ...: "
                          "that many self-training rounds)")
     ap.add_argument("--screen-full", action="store_true",
@@ -411,7 +411,8 @@ def _learned_section(dev, n_train, n_eval):
     """The learned half of the metric on the screening shapes (the 8,000-atom receptor, 30 A box, 81^3 x 8 maps;
     ligands with 8-80 heavy atoms and 0-20 torsions), at reduced ligand counts: the proposal network is trained on
     the plain search's own moves from n_train fresh ligands (two self-training rounds, <= 2 M logged moves per
-    collection; 4 candidate targets per learned step; 3-component translation mixture), then FP16 maps + learned
+    collection; 4 candidate targets per learned step; 3-component translation mixture; 60 % of the steps learned
+    before step 64, 30 % after), then FP16 maps + learned
     proposal and plain FP32 dock n_eval held-out ligands x 32 chains from the same Stage-A starts at several step
     budgets. Gap = a ligand's best energy minus the lowest energy any run
     found for it (an 8,000-step plain run included). Reported: ligands/s and energy evaluations/s of each method
@@ -423,7 +424,7 @@ def _learned_section(dev, n_train, n_eval):
     held = synth.ligand_set(n_eval, (8, 80), (0, 20), seed0=400_000)
     t0 = time.perf_counter()
     ab = ab_compare(rec2, train, held, device=dev, budgets=(250, 500, 1000, 2000, 4000),
-                    learned=[("learned_f16", 32, 0.3, "dagger2", 4, False, 3)], log_cap=2_000_000,
+                    learned=[("learned_f16", 32, (0.6, 0.3, 64), "dagger2", 4, False, 3)], log_cap=2_000_000,
                     learned_budgets=(250, 500, 1000, 2000), plain_f16=False)
     wall = time.perf_counter() - t0
     interp = ab.get("interp_at_gap_0.1", {})
@@ -442,7 +443,8 @@ def _learned_section(dev, n_train, n_eval):
     net_share = (sum(r["net_ms"] for r in lr) / sum(r["net_ms"] + r["mc_segments_ms"] for r in lr)) if lr else None
     return {"workload": (f"screening shapes: 8000-atom receptor, 30 A box, 81^3 x 8 maps; {n_eval} held-out ligands "
                          f"(8-80 heavy atoms, 0-20 torsions) x 32 chains; proposal trained on {n_train} fresh "
-                         f"ligands (2 self-training rounds, 3-component translation mixture, 4 tries per learned step)"),
+                         f"ligands (2 self-training rounds, 3-component translation mixture, 4 tries per learned step, "
+                         f"learned fraction 0.6 before step 64 and 0.3 after)"),
             "gap_bar_kcal_mol": 0.1, "plain_f32": plain, "learned_f16": learned,
             "speedup_ligands_per_s_at_gap_0.1": (learned["ligands_per_s"] / plain["ligands_per_s"]
                                                  if plain and learned else None),
