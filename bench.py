@@ -370,17 +370,6 @@ def run_ours(args, rank, world, local_rank):
            "mc_autotune": __import__("adock_b200.autotune", fromlist=["cached"]).cached()}
     if rank == 0 and world == 1 and not args.no_extras:
         out["grid_and_precision"] = _grid_and_precision(dev, ligs)
-    from adock_b200.proposal import parse_frac
-
-    def parse_variants(spec):
-        out_v = []
-        for v in spec.split(","):
-            f = v.split(":")
-            out_v.append((f[0], int(f[1]), parse_frac(f[2])) + ((f[3],) if len(f) > 3 else ())
-                         + ((int(f[4]),) if len(f) > 4 else ()) + ((f[5] in ("1", "hint"),) if len(f) > 5 else ())
-                         + ((int(f[6]),) if len(f) > 6 else ()))
-        return out_v
-
     variants = parse_variants(args.ab_variants)
     if rank == 0 and world == 1 and args.ab:
         from adock_b200 import synth
@@ -523,6 +512,21 @@ def _cpu_baseline(ligs, rec, cfg):
                       f"{cfg['mc_steps']} steps, one full stock search, {dt:.1f} s"}
 
 
+def parse_variants(spec):
+    """Learned variants from "name:segment_steps:fraction[:training[:tries[:hint[:n_comp]]]],..." (fraction "0.3"
+    or "0.6>0.3@64") as the tuples ``proposal.parse_learned`` reads."""
+    from adock_b200.proposal import parse_frac
+    out_v = []
+    for v in spec.split(","):
+        if not v:
+            continue
+        f = v.split(":")
+        out_v.append((f[0], int(f[1]), parse_frac(f[2])) + ((f[3],) if len(f) > 3 else ())
+                     + ((int(f[4]),) if len(f) > 4 else ()) + ((f[5] in ("1", "hint"),) if len(f) > 5 else ())
+                     + ((int(f[6]),) if len(f) > 6 else ()))
+    return out_v
+
+
 def run_screen_full(args):
     """The full-form screening workload (configs of the screening run: FP16 maps, learned proposal, 32 chains per
     ligand, ligands with 8-80 heavy atoms and 0-20 torsions against the 8,000-atom receptor) as one batch, against
@@ -531,18 +535,14 @@ def run_screen_full(args):
     import numpy as np
     import torch
     from adock_b200 import params, synth
-    from adock_b200.proposal import full_screen, parse_frac
+    from adock_b200.proposal import full_screen
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
     rec2 = synth.config_receptor(2)
     nw = min(16, os.cpu_count() or 1)     # the generator is Python; the seeds are split over processes
     train = synth.ligand_set(args.screen_train, (8, 80), (0, 20), seed0=300_000, workers=nw)
     ligs = synth.ligand_set(args.screen_full_ligands, (8, 80), (0, 20), seed0=700_000, workers=nw)
-    variant = next(v for v in args.screen_variants.split(",") if v)
-    f = variant.split(":")
-    variant = (f[0], int(f[1]), parse_frac(f[2])) + ((f[3],) if len(f) > 3 else ()) + \
-        ((int(f[4]),) if len(f) > 4 else ()) + ((f[5] in ("1", "hint"),) if len(f) > 5 else ()) + \
-        ((int(f[6]),) if len(f) > 6 else ())
+    variant = parse_variants(args.screen_variants)[0]
     clocks = ClockSampler(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0])
     t0 = time.perf_counter()
     steps_l = tuple(int(x) for x in args.screen_full_learned_steps.split(",") if x)
