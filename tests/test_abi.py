@@ -83,3 +83,23 @@ def test_pipeline_entry_points_reject_bad_arguments_without_gpu():
         _lib.call("adock_grid_vina_cells", p, p, 10, p, ctypes.addressof(dims), ctypes.addressof(org), 1.0,
                   ctypes.addressof(rad), ctypes.addressof(tab), ctypes.addressof(tab), ctypes.addressof(tab), 18,
                   ctypes.addressof(lt), 1, 0.0, 0.0, 0.0, 0.375, 8, 8, 8, ctypes.addressof(prm), 0, p, None)
+
+
+def test_proposal_entry_points_reject_bad_arguments_without_gpu():
+    """The proposal kernels' host checks: only 1 or 3 translation components, at most 512 targets per chain, and
+    no ligand-best hint without its key scratch."""
+    from adock_b200 import _lib
+    if not _lib.LIB_PATH.exists():
+        pytest.skip("libadock_b200.so not built")
+    p = ctypes.c_void_p(8)      # never dereferenced: every call below fails its argument check first
+    with pytest.raises(RuntimeError, match="n_comp"):
+        _lib.call("adock_mlp_nll", p, p, 4, 2, p, p, None)
+    lig = _lib.Ligands()
+    w = _lib.Work()
+    w.info = 8
+    with pytest.raises(RuntimeError, match="n_comp"):
+        _lib.call("adock_prop_sample", lig, w, p, p, 4, p, p, 27, 32, 2, 1, 0, p, None)
+    with pytest.raises(RuntimeError, match="512"):
+        _lib.call("adock_prop_sample", lig, w, p, p, 4, p, p, 27, 600, 1, 1, 0, p, None)
+    with pytest.raises(RuntimeError, match="null"):
+        _lib.call("adock_prop_hint", 4, 8, p, p, 27, p, None, p, None)
