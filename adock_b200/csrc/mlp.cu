@@ -1,8 +1,10 @@
 // Proposal network kernels (sm_100a): BF16 GEMM on the tensor cores with FP32 accumulation and fused epilogues,
 // Gaussian negative log-likelihood + its gradient, SiLU backward, bias-gradient reduction, Adam.
 //
-// Network: x [288] -> SiLU(W1 x + b1) [256] -> SiLU(W2 h1 + b2) [256] -> W3 h2 + b3 [64]. Output columns 0..25 are
-// the means and 32..57 the log standard deviations of the move (translation 3, rotation vector 3, torsions 20).
+// Network: x [320] -> SiLU(W1 x + b1) [256] -> SiLU(W2 h1 + b2) [256] -> W3 h2 + b3 [64]. Output columns 0..25 are
+// the means and 32..57 the log standard deviations of the move (translation 3, rotation vector 3, torsions 20);
+// with a translation mixture, columns 27..29 and 58..60 hold two more translation means and 26, 30, 61 the
+// mixing logits.
 //
 // GEMM: C[M,N] = A[M,K] B[K,N] with A and B in BF16 at arbitrary (row, column) strides, so the same kernel serves
 // the forward pass (X W), the input gradient (dY W^T) and the weight gradient (X^T dY). adock_gemm_bf16 runs it on
