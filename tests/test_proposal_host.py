@@ -92,3 +92,35 @@ def test_learned_fraction_schedule():
     assert sched == (0.5, 0.3, 128)
     assert [frac_at(sched, s) for s in (0, 96, 128, 500)] == [0.5, 0.5, 0.3, 0.3]
     assert frac_at(0.3, 1000) == 0.3
+
+
+def test_interp_to_gap_between_budgets():
+    """Steps to a median gap by log-log interpolation between the two bracketing budgets, ligands/s from the time
+    per ligand interpolated linearly in steps; the first budget when it already reaches the gap; None when none
+    does."""
+    from adock_b200.proposal import interp_to_gap
+    rows = [{"steps": 250, "median_gap": 0.4, "ligands_per_s": 160.0},
+            {"steps": 500, "median_gap": 0.1 / 4, "ligands_per_s": 80.0},
+            {"steps": 1000, "median_gap": 0.01, "ligands_per_s": 40.0}]
+    r = interp_to_gap(rows, 0.1)
+    # log gap falls by log(16) over log(2) steps: 0.1 is a quarter of that way
+    assert math.isclose(r["steps"], 250 * 2 ** 0.5, rel_tol=1e-9)
+    w = (r["steps"] - 250) / 250
+    assert math.isclose(r["ligands_per_s"], 1 / ((1 - w) / 160 + w / 80), rel_tol=1e-9)
+    assert interp_to_gap(rows, 0.5) == {"steps": 250, "ligands_per_s": 160.0}
+    assert interp_to_gap(rows, 0.001) is None
+
+
+def test_parse_learned_and_bench_specs():
+    import importlib.util
+    import pathlib
+    from adock_b200.proposal import parse_learned
+    v = parse_learned([("a", 32, 0.3), ("b", 32, (0.6, 0.3, 64), "dagger2", 4, False, 3)])
+    assert v["a"] == (32, 0.3, "chain", 1, False, 1)
+    assert v["b"] == (32, (0.6, 0.3, 64), "dagger2", 4, False, 3)
+    path = pathlib.Path(__file__).resolve().parents[1] / "bench.py"
+    spec = importlib.util.spec_from_file_location("bench_for_test", path)
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    got = bench.parse_variants("learned_dagger2:32:0.6>0.3@64:dagger2:4:0:3,x:16:0.5:chain:1:hint")
+    assert got == [("learned_dagger2", 32, (0.6, 0.3, 64), "dagger2", 4, False, 3), ("x", 16, 0.5, "chain", 1, True)]
